@@ -1,0 +1,350 @@
+#!/usr/bin/env python3
+"""Benchmark of the copy-model preferential-attachment generator.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c3]
+    python bench.py --impl reference ...
+
+One step = one generation of the whole graph (pa_generate: the scratch clear
+and the persistent generator launch) into buffers already resident in HBM.
+Metric: edges/s (whole job).  The default workload is the largest single-GPU
+configuration: n = 2^30 nodes, d = 4, p = 0.5, int64 ids, (d+1)-clique seed,
+Philox seed 1234 -- 4,294,967,286 edges, 68.7 GB of (src, dst) pairs.  The
+output alone is ~545x the 126 MB L2, so no L2 flush is needed between steps.
+
+Multi-GPU (torchrun, N > 1): one graph does not shard (every copy read may hit
+any earlier node), so each rank generates its own full replica and `value`
+counts the edges of all ranks over the slowest rank's time (weak scaling).
+
+Besides the device-timed value the line carries:
+  e2e          the same generation through the C ABI from host parameters,
+               host-timed, including the device->host read of each step's
+               result block (status and counters);
+  roofline     algorithmic bytes of the generator kernel per launch over its
+               CUDA-event duration, against the measured HBM copy bandwidth;
+  cpu_baseline the sequential CPU oracle on a bounded sample (1 core);
+  clocks       SM clocks and throttle reasons sampled during the timed region.
+
+--impl reference times the reference's own sequential generator
+(oracle/_ref/scm_ref, src/PA/SPA/SerialCopyModel3.cpp compiled from the
+reference sources) on a bounded sample per step; where that binary is absent
+it falls back to the CPU oracle restatement.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cuppa-public_b200"))
+
+CLIQUE, STAR_REF = 1, 0
+WORKLOADS = {
+    "c3": dict(n=2 ** 30, d=4, p=0.5, seed=1234, id_bits=64, seed_mode=CLIQUE,
+               name="copy-model PA, n=2^30, d=4, p=0.5, int64 ids, clique seed, Philox seed 1234"),
+    "c3p0": dict(n=2 ** 30, d=4, p=0.0, seed=1234, id_bits=64, seed_mode=CLIQUE,
+                 name="copy-model PA, n=2^30, d=4, p=0.0, int64 ids, clique seed, Philox seed 1234"),
+    "c2": dict(n=10 ** 8, d=16, p=0.5, seed=7, id_bits=64, seed_mode=CLIQUE,
+               name="copy-model PA, n=10^8, d=16, p=0.5, int64 ids, clique seed, Philox seed 7"),
+    "c3s": dict(n=2 ** 25, d=4, p=0.5, seed=1234, id_bits=64, seed_mode=CLIQUE,
+                name="copy-model PA, n=2^25, d=4, p=0.5, int64 ids, clique seed, Philox seed 1234 "
+                     "(profiling size)"),
+    "c1": dict(n=10 ** 5, d=4, p=0.5, seed=42, id_bits=32, seed_mode=CLIQUE,
+               name="copy-model PA, n=10^5, d=4, p=0.5, int32 ids, clique seed, Philox seed 42"),
+}
+METRIC = "edges/s on 1 B200 (copy-model PA generation)"
+CPU_SAMPLE_NODES = 2 ** 24      # oracle sample: ~67M edges, a few seconds on one core
+REF_SAMPLE_NODES = 2 ** 23      # reference scm sample per step: ~33.5M edges
+
+
+def algorithmic_bytes_per_edge(w) -> float:
+    """2s (pair write) + (1-p)s (copy-target read), s = id bytes."""
+    s = w["id_bits"] // 8
+    return 2 * s + (1.0 - w["p"]) * s
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic(workload: str):
+    """Per-launch DRAM bytes of the generator kernel from a committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "gen_kernel_traffic.json")
+    try:
+        with open(path) as f:
+            t = json.load(f)
+        return t.get(workload, {}).get("dram_bytes_per_launch")
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 200 ms while running."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline_oracle(w, nodes: int):
+    """The sequential oracle (1 core) on `nodes` nodes of the same (d, p, seed)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle as orc
+    n = min(nodes, w["n"])
+    t0 = time.perf_counter()
+    orc.generate(n, w["d"], w["p"], w["seed"], w["seed_mode"])
+    dt = time.perf_counter() - t0
+    edges = orc.edge_count(n, w["d"], w["seed_mode"])
+    return {"value": edges / dt, "unit": "edges/s", "cores": 1, "kind": "port",
+            "sample": f"oracle (Philox restatement of SerialCopyModel3.cpp), n={n}, d={w['d']}, "
+                      f"p={w['p']}, {edges} edges in {dt:.2f} s, one thread"}
+
+
+def run_reference(args, w):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    ref = os.path.join(ROOT, "oracle", "_ref", "scm_ref")
+    n = REF_SAMPLE_NODES
+    d = w["d"]
+    edges = (n - d - 1) * d + d
+    times = []
+    if os.path.exists(ref):
+        kind = "reference"
+        sample = (f"reference -A scm (SerialCopyModel3.cpp, MT19937-64, star seed, int32 ids), "
+                  f"n={n}, d={d}, p={w['p']}; its own 'Computation Time' per step; single-threaded")
+        with tempfile.TemporaryDirectory() as td:
+            for i in range(args.warmup + args.steps):
+                out = subprocess.run([ref, str(n), str(d), str(w["p"]), td, "-"], cwd=td,
+                                     capture_output=True, text=True, check=True).stdout
+                t = [float(x.split(":")[1]) for x in out.splitlines()
+                     if x.startswith("Computation Time")][0]
+                if i >= args.warmup:
+                    times.append(t)
+    else:
+        kind = "port"
+        sample = f"oracle restatement (reference binary absent), n={n}, d={d}, p={w['p']}"
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import _oracle as orc
+        edges = orc.edge_count(n, d, w["seed_mode"])
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            orc.generate(n, d, w["p"], w["seed"], w["seed_mode"])
+            if i >= args.warmup:
+                times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = edges * len(times) / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "edges/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64" if w["id_bits"] == 64 else "int32",
+        "data": "synthetic (generator parameters only)",
+        "config": {"workload": w["name"], "sample_nodes": n},
+        "cpu_baseline": {"value": value, "unit": "edges/s", "cores": 1, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_gpu(args, w):
+    import torch
+    import torch.distributed as dist
+    import cuppa_b200 as pa
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    prm = pa.make_params(w["n"], w["d"], w["p"], seed=w["seed"], id_bits=w["id_bits"],
+                         seed_mode=w["seed_mode"], tile_passes=args.tile_passes,
+                         blocks=args.blocks)
+    E = pa.edge_count(prm)
+    edges, scratch = pa.alloc_buffers(prm)
+    stream = torch.cuda.Stream()
+
+    def step():
+        pa.generate_into(prm, edges, scratch, stream)
+
+    # warm-up (each checked)
+    for _ in range(args.warmup):
+        step()
+        st = pa.finish(scratch, stream)
+        pa.check(st.status, "warm-up generation")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-timed region
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    t_all0, t_all1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(local) as clk:
+        t_all0.record(stream)
+        for i in range(args.steps):
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+        t_all1.record(stream)
+        stream.synchronize()
+    barrier()
+    st = pa.finish(scratch, stream)
+    pa.check(st.status, "timed generation")
+    ms = t_all0.elapsed_time(t_all1)
+    launch_ms = [a.elapsed_time(b) for a, b in ev]
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * E * args.steps / (ms / 1e3)
+
+    # ---- end to end through the C ABI: host params -> generation -> result read
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        pa.generate_into(prm, edges, scratch, stream)
+        st = pa.finish(scratch, stream)          # stream sync + device->host result block
+    t1 = time.perf_counter()
+    pa.check(st.status, "e2e generation")
+    e2e_s = t1 - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * E * args.steps / e2e_s, "unit": "edges/s",
+           "h2d_bytes_per_step": ctypes_sizeof_params(pa), "d2h_bytes_per_step": 64}
+
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        bpe = algorithmic_bytes_per_edge(w)
+        kern_s = statistics.mean(launch_ms) / 1e3
+        achieved = E * bpe / kern_s / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int64" if w["id_bits"] == 64 else "int32",
+            "data": "synthetic (generator parameters only; output is the graph)",
+            "config": {"workload": w["name"], "edges": E,
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": f"output {E * 2 * w['id_bits'] // 8 / 1e9:.1f} GB > 126 MB L2; "
+                             "no flush needed"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "bytes_per_edge": bpe, "traffic": load_traffic(args.workload),
+                         "kernel": "gen_kernel", "launch_ms_mean": kern_s * 1e3},
+            "e2e": e2e,
+            "gpu_launches": args.steps,
+            "clocks": clk.summary(),
+            "device_stats": st.as_dict(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_oracle(w, CPU_SAMPLE_NODES)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def ctypes_sizeof_params(pa) -> int:
+    import ctypes
+    return ctypes.sizeof(pa.PaParams)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c3")
+    ap.add_argument("--tile-passes", type=int, default=0)
+    ap.add_argument("--blocks", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference(args, w)
+    return run_gpu(args, w)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,139 @@
+// pa_post.cu -- passes over a generated edge list: row canonicalisation and
+// undirected degrees (the device side of src/PA/cuPPA/cuPPA.cu:103-165, which
+// copies the whole graph to the host and counts there).
+#include "pa_device.cuh"
+#include "pa_internal.h"
+
+namespace pa {
+namespace {
+
+constexpr uint32_t kFull = 0xffffffffu;
+
+// Sort each generated node's d pairs by dst.  A group of d lanes holds one row;
+// lane i's rank is the number of smaller values in its group (values in a row
+// are distinct), and it stores its pair at that rank.  All loads of a warp
+// iteration happen before its stores, so in == out is safe.
+template <typename Id>
+__global__ void canon_kernel(const Id *in, Id *out, uint64_t n, uint32_t d, uint64_t seed_edges)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t G = 32u / d;
+    const uint32_t g = lane / d, i = lane - g * d;
+    const bool used = lane < G * d;
+    const uint64_t rows = n - (d + 1);
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    const uint64_t w0 = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+
+    // seed edges are already canonical
+    if (in != out)
+        for (uint64_t e = w0 * 32 + lane; e < seed_edges; e += warps * 32) {
+            out[2 * e] = in[2 * e];
+            out[2 * e + 1] = in[2 * e + 1];
+        }
+
+    for (uint64_t r0 = w0 * G; r0 < rows; r0 += warps * G) {
+        const uint64_t row = r0 + g;
+        const bool act = used && row < rows;
+        const uint64_t e = seed_edges + row * d + i;
+        Id src = 0, dst = 0;
+        if (act) {
+            src = in[2 * e];
+            dst = in[2 * e + 1];
+        }
+        uint32_t rank = 0;
+        for (uint32_t j = 0; j < d; ++j) {
+            const Id o = __shfl_sync(kFull, dst, g * d + j);
+            rank += (o < dst) ? 1u : 0u;
+        }
+        __syncwarp();
+        if (act) {
+            const uint64_t eo = seed_edges + row * d + rank;
+            out[2 * eo] = src;
+            out[2 * eo + 1] = dst;
+        }
+    }
+}
+
+// Undirected degree: +1 on both endpoints of every pair.  Equal endpoints in a
+// warp are combined with __match_any_sync before the atomic (hub nodes take
+// most increments when p is small).
+template <typename Id>
+__global__ void degree_kernel(const Id *E, uint64_t n_edges, uint64_t n, unsigned long long *deg)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n_edges; base += stride) {
+        const uint64_t e = base + threadIdx.x;
+        unsigned long long s = e < n_edges ? (unsigned long long)E[2 * e] : ~0ull;
+        unsigned long long t = e < n_edges ? (unsigned long long)E[2 * e + 1] : ~0ull;
+        const bool act = s < n && t < n;   // ids are used as addresses: never trust them
+        if (!act) s = t = ~0ull - lane;    // unique keys, never a leader for a real id
+        const uint32_t ms = __match_any_sync(kFull, s);
+        const uint32_t mt = __match_any_sync(kFull, t);
+        if (act && (__ffs(ms) - 1) == (int)lane) atomicAdd(deg + s, (unsigned long long)__popc(ms));
+        if (act && (__ffs(mt) - 1) == (int)lane) atomicAdd(deg + t, (unsigned long long)__popc(mt));
+    }
+}
+
+int grid_for(uint64_t work_items, uint32_t threads)
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    uint64_t want = (work_items + threads - 1) / threads;
+    const uint64_t cap = (uint64_t)sms * 8;
+    if (want > cap) want = cap;
+    return (int)(want ? want : 1);
+}
+
+}  // namespace
+}  // namespace pa
+
+using namespace pa;
+
+extern "C" {
+
+int pa_canonicalize(const pa_params *prm, const void *d_edges, void *d_out, void *stream)
+{
+    GenPlan p;
+    const int rc = make_plan(prm, &p);
+    if (rc != PA_OK) return rc;
+    if (!d_edges || !d_out) return PA_ERR_INVALID;
+    const uint64_t rows = prm->n - p.u_first;
+    const uint32_t threads = 256;
+    const int grid = grid_for(rows * prm->d, threads);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (p.id_bytes == 8)
+        canon_kernel<int64_t><<<grid, threads, 0, s>>>((const int64_t *)d_edges, (int64_t *)d_out,
+                                                       prm->n, prm->d, p.seed_edges);
+    else
+        canon_kernel<int32_t><<<grid, threads, 0, s>>>((const int32_t *)d_edges, (int32_t *)d_out,
+                                                       prm->n, prm->d, p.seed_edges);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PA_OK : set_cuda_error(e);
+}
+
+int pa_degrees(const pa_params *prm, const void *d_edges, int64_t *d_deg, void *stream)
+{
+    GenPlan p;
+    const int rc = make_plan(prm, &p);
+    if (rc != PA_OK) return rc;
+    if (!d_edges || !d_deg) return PA_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemsetAsync(d_deg, 0, prm->n * sizeof(int64_t), s);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    const uint32_t threads = 256;
+    const int grid = grid_for(p.n_edges, threads);
+    if (p.n_edges) {
+        if (p.id_bytes == 8)
+            degree_kernel<int64_t><<<grid, threads, 0, s>>>((const int64_t *)d_edges, p.n_edges,
+                                                            prm->n, (unsigned long long *)d_deg);
+        else
+            degree_kernel<int32_t><<<grid, threads, 0, s>>>((const int32_t *)d_edges, p.n_edges,
+                                                            prm->n, (unsigned long long *)d_deg);
+    }
+    e = cudaGetLastError();
+    return e == cudaSuccess ? PA_OK : set_cuda_error(e);
+}
+
+}  // extern "C"

@@ -1,0 +1,315 @@
+"""Python binding of the B200 copy-model preferential-attachment generator.
+
+The product is the C ABI in ``include/cuppa_pa.h`` (``lib/libcuppa_pa.so``);
+this module binds it with ctypes and uses torch only for device memory and
+streams.  There is no CPU fallback: if the shared library is missing or no CUDA
+device is present, calls fail with an exception.
+
+The host-side interface mirrors the reference's (paths relative to the
+cuPPA-Public tree):
+
+* ``cuPPA(nNodes, mEdgesPerNode, p)`` with ``generateGraph(conf)``,
+  ``generateGraphAdaptive(conf)`` and ``printDegreeDistribution(conf)``
+  -- ``src/PA/cuPPA/cuPPA.cuh:84-105``;
+* ``ExperimentConfiguration`` with the reference field names
+  (``_n1``, ``_x1``, ``_alpha``, ``_blockSize``, ``_threadsPerBlock``,
+  ``_stages``, ``_FLAG_SHOW_DEGREE_DISTRIBUTION``, ``_distfile1``,
+  ``_outputDir``) -- ``src/Utility/ExperimentConfiguration.hpp:51-96``,
+  plus the new ``seed``, ``id_bits`` and ``seed_mode``.
+
+Where the reference exits the process on a CUDA error
+(``src/Common/CommonHelper.cuh:148-157``) this binding raises ``CuppaError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import os
+from typing import Optional
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libcuppa_pa.so")
+
+PA_OK = 0
+PA_ERR_INVALID = 1
+PA_ERR_OOM = 2
+PA_ERR_SPIN_TIMEOUT = 3
+PA_ERR_CUDA = 4
+PA_ERR_CAPACITY = 5
+PA_ERR_NOT_SUPPORTED = 6
+PA_ERR_BUSY = 7
+PA_ERR_NOT_FOUND = 8
+
+PA_SEED_STAR_REF = 0
+PA_SEED_CLIQUE = 1
+PA_LAYOUT_PAIRS = 0
+
+# Test-only: the generator never publishes its first tile, so every wait on it
+# runs into the wait limit (a flag that nothing sets).
+PA_FLAG_TEST_WITHHOLD_FIRST_TILE = 1 << 31
+
+
+class CuppaError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        self.status = status
+        super().__init__(f"{where}: {strerror(status)} (status {status})")
+
+
+class PaParams(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_uint64),
+        ("d", ctypes.c_uint32),
+        ("id_bits", ctypes.c_uint32),
+        ("p", ctypes.c_double),
+        ("seed", ctypes.c_uint64),
+        ("seed_mode", ctypes.c_uint32),
+        ("layout", ctypes.c_uint32),
+        ("blocks", ctypes.c_uint32),
+        ("threads", ctypes.c_uint32),
+        ("tile_passes", ctypes.c_uint32),
+        ("flags", ctypes.c_uint32),
+        ("spin_limit_ns", ctypes.c_uint64),
+    ]
+
+
+class PaStats(ctypes.Structure):
+    _fields_ = [
+        ("retries", ctypes.c_uint64),
+        ("waits", ctypes.c_uint64),
+        ("tiles", ctypes.c_uint64),
+        ("status", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class PaGraph(ctypes.Structure):
+    _fields_ = [
+        ("params", PaParams),
+        ("edges", ctypes.c_void_p),
+        ("n_edges", ctypes.c_uint64),
+        ("edges_bytes", ctypes.c_uint64),
+        ("scratch", ctypes.c_void_p),
+        ("scratch_bytes", ctypes.c_uint64),
+    ]
+
+
+_lib: Optional[ctypes.CDLL] = None
+
+_P = ctypes.POINTER
+_SIGS = {
+    "pa_abi_version": (ctypes.c_int, []),
+    "pa_last_cuda_error": (ctypes.c_int, []),
+    "pa_strerror": (ctypes.c_char_p, [ctypes.c_int]),
+    "pa_params_init": (ctypes.c_int, [_P(PaParams)]),
+    "pa_params_check": (ctypes.c_int, [_P(PaParams)]),
+    "pa_seed_edge_count": (ctypes.c_uint64, [ctypes.c_uint32, ctypes.c_uint32]),
+    "pa_edge_count": (ctypes.c_uint64, [_P(PaParams)]),
+    "pa_edges_bytes": (ctypes.c_int, [_P(PaParams), _P(ctypes.c_uint64)]),
+    "pa_scratch_bytes": (ctypes.c_int, [_P(PaParams), _P(ctypes.c_uint64)]),
+    "pa_generate": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_uint64,
+                                   ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),
+    "pa_generate_finish": (ctypes.c_int, [ctypes.c_void_p, _P(PaStats), ctypes.c_void_p]),
+    "pa_canonicalize": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p]),
+    "pa_degrees": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_void_p,
+                                  ctypes.c_void_p]),
+    "pa_graph_create": (ctypes.c_int, [_P(PaParams), _P(PaGraph)]),
+    "pa_graph_generate": (ctypes.c_int, [_P(PaGraph), ctypes.c_void_p, _P(PaStats)]),
+    "pa_graph_destroy": (ctypes.c_int, [_P(PaGraph)]),
+}
+
+
+def lib() -> ctypes.CDLL:
+    """Load libcuppa_pa.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(
+                f"{LIB_PATH} is missing: build it with `make -C cuppa-public_b200`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def strerror(status: int) -> str:
+    try:
+        return lib().pa_strerror(status).decode()
+    except Exception:  # pragma: no cover - only when the library is absent
+        return f"status {status}"
+
+
+def check(status: int, where: str) -> None:
+    if status != PA_OK:
+        raise CuppaError(status, where)
+
+
+def make_params(n: int, d: int, p: float, seed: int = 42, id_bits: int = 32,
+                seed_mode: int = PA_SEED_CLIQUE, blocks: int = 0, threads: int = 0,
+                tile_passes: int = 0, flags: int = 0, spin_limit_ns: int = 0) -> PaParams:
+    prm = PaParams()
+    check(lib().pa_params_init(ctypes.byref(prm)), "pa_params_init")
+    prm.n, prm.d, prm.p, prm.seed = n, d, float(p), seed
+    prm.id_bits, prm.seed_mode = id_bits, seed_mode
+    prm.blocks, prm.threads, prm.tile_passes = blocks, threads, tile_passes
+    prm.flags, prm.spin_limit_ns = flags, spin_limit_ns
+    return prm
+
+
+def edge_count(prm: PaParams) -> int:
+    return int(lib().pa_edge_count(ctypes.byref(prm)))
+
+
+def sizes(prm: PaParams) -> tuple[int, int]:
+    """(edge buffer bytes, scratch bytes) for prm."""
+    eb, sb = ctypes.c_uint64(), ctypes.c_uint64()
+    check(lib().pa_edges_bytes(ctypes.byref(prm), ctypes.byref(eb)), "pa_edges_bytes")
+    check(lib().pa_scratch_bytes(ctypes.byref(prm), ctypes.byref(sb)), "pa_scratch_bytes")
+    return int(eb.value), int(sb.value)
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("cuppa_b200 needs a CUDA device; there is no CPU fallback")
+    return torch
+
+
+def _stream_ptr(stream) -> int:
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+def alloc_buffers(prm: PaParams, device=None):
+    """Device tensors for the edges (E x 2 ids) and the generation scratch."""
+    torch = _torch()
+    eb, sb = sizes(prm)
+    dt = torch.int64 if prm.id_bits == 64 else torch.int32
+    E = edge_count(prm)
+    edges = torch.empty((max(E, 1), 2), dtype=dt, device=device or "cuda")
+    scratch = torch.empty(max(sb, 256), dtype=torch.uint8, device=device or "cuda")
+    return edges, scratch
+
+
+def generate_into(prm: PaParams, edges, scratch, stream=None) -> None:
+    """Stream-ordered pa_generate into the given device tensors."""
+    rc = lib().pa_generate(ctypes.byref(prm), ctypes.c_void_p(edges.data_ptr()),
+                           edges.numel() * edges.element_size(),
+                           ctypes.c_void_p(scratch.data_ptr()), scratch.numel(),
+                           ctypes.c_void_p(_stream_ptr(stream)))
+    check(rc, "pa_generate")
+
+
+def finish(scratch, stream=None) -> PaStats:
+    st = PaStats()
+    lib().pa_generate_finish(ctypes.c_void_p(scratch.data_ptr()), ctypes.byref(st),
+                             ctypes.c_void_p(_stream_ptr(stream)))
+    return st
+
+
+def generate(prm: PaParams, stream=None, raise_on_error: bool = True):
+    """Generate one graph; returns (edges tensor [E, 2] on the device, PaStats)."""
+    edges, scratch = alloc_buffers(prm)
+    generate_into(prm, edges, scratch, stream)
+    st = finish(scratch, stream)
+    if raise_on_error:
+        check(st.status, "pa_generate (device)")
+    return edges[: edge_count(prm)], st
+
+
+def canonicalize(prm: PaParams, edges, out=None, stream=None):
+    out = edges if out is None else out
+    check(lib().pa_canonicalize(ctypes.byref(prm), ctypes.c_void_p(edges.data_ptr()),
+                                ctypes.c_void_p(out.data_ptr()),
+                                ctypes.c_void_p(_stream_ptr(stream))), "pa_canonicalize")
+    return out
+
+
+def degrees(prm: PaParams, edges, stream=None):
+    torch = _torch()
+    deg = torch.empty(prm.n, dtype=torch.int64, device=edges.device)
+    check(lib().pa_degrees(ctypes.byref(prm), ctypes.c_void_p(edges.data_ptr()),
+                           ctypes.c_void_p(deg.data_ptr()),
+                           ctypes.c_void_p(_stream_ptr(stream))), "pa_degrees")
+    return deg
+
+
+def degree_distribution_csv(deg) -> str:
+    """'Degree,Count' CSV of src/PA/cuPPA/cuPPA.cu:150-157 (degree-0 nodes skipped)."""
+    torch = _torch()
+    vals, cnts = torch.unique(deg[deg > 0], return_counts=True)
+    rows = ["Degree,Count"] + [f"{int(v)},{int(c)}" for v, c in zip(vals.tolist(), cnts.tolist())]
+    return "\n".join(rows) + "\n"
+
+
+# ---------------------------------------------------------------------------
+# Mirror of the reference's host interface
+# ---------------------------------------------------------------------------
+@dataclasses.dataclass
+class ExperimentConfiguration:
+    """Reference field names (src/Utility/ExperimentConfiguration.hpp:51-96)
+    with the runner defaults of src/main.cu:130-174, plus seed/id width/seed mode."""
+    _algorithm: str = "cuppa"
+    _n1: int = 1000
+    _x1: int = 4
+    _alpha: float = 0.5
+    _stages: int = 1000
+    _blockSize: int = 0          # -b: 0 = one full wave of the GPU
+    _threadsPerBlock: int = 0    # -t: 0 = auto
+    _warpSize: int = 32
+    _FLAG_SHOW_DEGREE_DISTRIBUTION: bool = False
+    _distfile1: str = "degreeDistribution.txt"
+    _outputDir: str = "./"
+    seed: int = 42
+    id_bits: int = 32
+    seed_mode: int = PA_SEED_CLIQUE
+
+
+class cuPPA:  # noqa: N801 - reference class name
+    """cuPPA(nNodes, mEdgesPerNode, p) -- src/PA/cuPPA/cuPPA.cuh:84-105.
+
+    Unlike the reference, the generated graph is kept (``self.edges``, a device
+    tensor of (u, v) pairs) instead of being freed before return
+    (src/PA/cuPPA/cuPPA_1.cu:519-522)."""
+
+    def __init__(self, nNodes: int, mEdgesPerNode: int, p: float):
+        self._N, self._M, self._p = int(nNodes), int(mEdgesPerNode), float(p)
+        self.edges = None
+        self.stats: Optional[PaStats] = None
+        self._prm: Optional[PaParams] = None
+
+    def _params(self, conf: ExperimentConfiguration) -> PaParams:
+        self._N, self._M, self._p = int(conf._n1), int(conf._x1), float(conf._alpha)
+        threads = conf._threadsPerBlock if conf._threadsPerBlock in (0, 256) else 0
+        return make_params(self._N, self._M, self._p, seed=conf.seed, id_bits=conf.id_bits,
+                           seed_mode=conf.seed_mode, blocks=conf._blockSize, threads=threads)
+
+    def generateGraph(self, conf: ExperimentConfiguration):
+        """cuPPA_1.cu:9 -- one persistent launch replaces the staged loop."""
+        self._prm = self._params(conf)
+        self.edges, self.stats = generate(self._prm)
+        if conf._FLAG_SHOW_DEGREE_DISTRIBUTION:
+            self.printDegreeDistribution(conf)
+        return self.edges
+
+    def generateGraphAdaptive(self, conf: ExperimentConfiguration):
+        """cuPPA_2.cu:9 -- the adaptive stage tuner has nothing to tune here."""
+        return self.generateGraph(conf)
+
+    def printDegreeDistribution(self, conf: ExperimentConfiguration) -> str:
+        """cuPPA.cu:103-165 -- degrees on the device, 'Degree,Count' CSV to
+        outputDir/distfile1."""
+        if self.edges is None:
+            raise RuntimeError("generateGraph first")
+        csv = degree_distribution_csv(degrees(self._prm, self.edges))
+        path = os.path.join(conf._outputDir, conf._distfile1)
+        with open(path, "w") as f:
+            f.write(csv)
+        return csv

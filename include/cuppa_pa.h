@@ -1,0 +1,143 @@
+/*
+ * cuppa_pa.h -- C ABI of the B200 copy-model preferential-attachment generator.
+ *
+ * Plain C, plain pointers and sizes; device buffers are CUDA device pointers and
+ * `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ * No call prints, exits, resets the device or frees memory it did not allocate.
+ * Every call returns a pa_status (0 = PA_OK).
+ *
+ * Reference interfaces replaced (paths relative to the cuPPA-Public tree):
+ *   class cuPPA(NodeType n, EdgeIndexType m, double p)     src/PA/cuPPA/cuPPA.cuh:84-105
+ *     .generateGraph(conf)          src/PA/cuPPA/cuPPA_1.cu:9-254   -> pa_generate
+ *     .generateGraphAdaptive(conf)  src/PA/cuPPA/cuPPA_2.cu:9-241   -> pa_generate
+ *                                   (the persistent launch needs no stage tuning)
+ *     .printDegreeDistribution      src/PA/cuPPA/cuPPA.cu:103-165   -> pa_degrees,
+ *                                   pa_degree_distribution
+ *   PAHelper::writeGraphToDisk      src/PA/SPA/PAHelper.hpp:163-177 -> pa_write_edges_text
+ *   runner flags -n -x -a -b -t -s  src/main.cu:188-213             -> pa_params fields
+ */
+#ifndef CUPPA_PA_H_
+#define CUPPA_PA_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PA_ABI_VERSION 1
+
+typedef enum pa_status {
+    PA_OK = 0,
+    PA_ERR_INVALID = 1,       /* a parameter is out of range or a pointer is NULL      */
+    PA_ERR_OOM = 2,           /* a device allocation made by the library failed        */
+    PA_ERR_SPIN_TIMEOUT = 3,  /* a device-side wait hit its limit (pa_params.spin_limit_ns) */
+    PA_ERR_CUDA = 4,          /* a CUDA runtime call failed; see pa_last_cuda_error()  */
+    PA_ERR_CAPACITY = 5,      /* a caller buffer is smaller than the call needs         */
+    PA_ERR_NOT_SUPPORTED = 6, /* valid request this build does not handle               */
+    PA_ERR_BUSY = 7,          /* server: admission refused for now (retry later)        */
+    PA_ERR_NOT_FOUND = 8      /* server: unknown or already released ticket             */
+} pa_status;
+
+/* Seed graph on nodes 0..d.
+ * STAR_REF: slots G[i][*] = i for i < d and G[d][j] = j -- the reference's seed
+ *           (src/PA/SPA/SerialCopyModel3.cpp:38-49, src/PA/cuPPA/cuPPA_RRP.cu:57-73);
+ *           its canonical edges are (d, j), j < d.
+ * CLIQUE:   nodes 0..d form K_{d+1}; G[v][*] = v's neighbours ascending. */
+enum { PA_SEED_STAR_REF = 0, PA_SEED_CLIQUE = 1 };
+
+/* Edge layouts.
+ * PAIRS: (src, dst) id pairs.  The first pa_seed_edge_count() pairs are the seed
+ *        rows' canonical edges (src > dst, sorted); then node u = d+1..n-1 owns the
+ *        d pairs at [S + (u-d-1)*d, S + (u-d)*d) in slot (generation) order.  Every
+ *        pair is an edge with src > dst.  This is the reference's G[N][M] slot array
+ *        (src/PA/cuPPA/cuPPA_1.cu:54) carried as an edge list. */
+enum { PA_LAYOUT_PAIRS = 0 };
+
+/* pa_params.flags.  TEST_WITHHOLD_FIRST_TILE is for tests of the wait limit:
+ * the generator never publishes its first tile, so every wait on that tile runs
+ * into spin_limit_ns and the call reports PA_ERR_SPIN_TIMEOUT. */
+#define PA_FLAG_TEST_WITHHOLD_FIRST_TILE 0x80000000u
+
+typedef struct pa_params {
+    uint64_t n;             /* nodes                        (-n/--n1; cuPPA(n, ...))      */
+    uint32_t d;             /* edges per new node, 1..32    (-x/--x1; M)                  */
+    uint32_t id_bits;       /* 32 or 64: width of each stored id                           */
+    double p;               /* probability of a direct pick (-a/--alpha), 0 <= p <= 1      */
+    uint64_t seed;          /* Philox key                                                 */
+    uint32_t seed_mode;     /* PA_SEED_*                                                  */
+    uint32_t layout;        /* PA_LAYOUT_*                                                */
+    uint32_t blocks;        /* -b: CTAs of the persistent launch; 0 = one wave of the GPU */
+    uint32_t threads;       /* -t: threads per CTA (multiple of 32, <= 1024); 0 = auto    */
+    uint32_t tile_passes;   /* warp passes per claimed tile (1, 2, 4 or 8); 0 = auto      */
+    uint32_t flags;         /* PA_FLAG_* (0 for normal use)                               */
+    uint64_t spin_limit_ns; /* limit of any single device wait; 0 = 2 s                    */
+} pa_params;
+
+/* Statistics and device-side status of one generation. */
+typedef struct pa_stats {
+    uint64_t retries;       /* draws rejected as duplicates                               */
+    uint64_t waits;         /* resolve iterations that waited on an unfinished tile       */
+    uint64_t tiles;         /* tiles completed                                            */
+    uint32_t status;        /* pa_status seen on the device (PA_OK or PA_ERR_SPIN_TIMEOUT) */
+    uint32_t reserved;
+} pa_stats;
+
+/* ---- sizes -------------------------------------------------------------- */
+/* Fills *out with defaults for every field; the caller then sets n, d, p, seed. */
+int pa_params_init(pa_params *out);
+/* Validate a parameter block (PA_OK or PA_ERR_INVALID / PA_ERR_NOT_SUPPORTED). */
+int pa_params_check(const pa_params *prm);
+uint64_t pa_seed_edge_count(uint32_t d, uint32_t seed_mode);
+/* Number of edges (pairs) the generator writes. */
+uint64_t pa_edge_count(const pa_params *prm);
+/* Bytes of the edge buffer and of the scratch buffer pa_generate needs. */
+int pa_edges_bytes(const pa_params *prm, uint64_t *bytes);
+int pa_scratch_bytes(const pa_params *prm, uint64_t *bytes);
+
+/* ---- generation ---------------------------------------------------------- */
+/* Stream-ordered generation into caller memory.  d_scratch (pa_scratch_bytes)
+ * is cleared by the call; it must not be shared by generations that overlap.
+ * Host-side errors return at once; device-side status is read by pa_generate_finish. */
+int pa_generate(const pa_params *prm, void *d_edges, uint64_t edges_bytes, void *d_scratch,
+                uint64_t scratch_bytes, void *stream);
+/* Wait for the stream, then copy the status and counters of the generation that
+ * last used d_scratch.  Returns the device status. */
+int pa_generate_finish(const void *d_scratch, pa_stats *out, void *stream);
+
+/* ---- post-processing ------------------------------------------------------ */
+/* Sort every node's d pairs by dst in place (or into d_out): the canonical edge
+ * list -- all (u, v) with u > v sorted by (u, v). */
+int pa_canonicalize(const pa_params *prm, const void *d_edges, void *d_out, void *stream);
+/* Undirected degree of every node: d_deg is int64[n]. */
+int pa_degrees(const pa_params *prm, const void *d_edges, int64_t *d_deg, void *stream);
+
+/* ---- convenience handle (library-owned memory) ----------------------------- */
+typedef struct pa_graph {
+    pa_params params;
+    void *edges;            /* device, edges_bytes                                        */
+    uint64_t n_edges;
+    uint64_t edges_bytes;
+    void *scratch;          /* device, scratch_bytes                                      */
+    uint64_t scratch_bytes;
+} pa_graph;
+
+/* Allocate edges + scratch on the current device for prm (no generation). */
+int pa_graph_create(const pa_params *prm, pa_graph *g);
+/* Generate into g on `stream` and wait; stats may be NULL. */
+int pa_graph_generate(pa_graph *g, void *stream, pa_stats *stats);
+/* Free what pa_graph_create allocated; safe on a zeroed handle. */
+int pa_graph_destroy(pa_graph *g);
+
+/* ---- errors --------------------------------------------------------------- */
+const char *pa_strerror(int status);
+/* The cudaError_t of the last PA_ERR_CUDA / PA_ERR_OOM on the calling thread. */
+int pa_last_cuda_error(void);
+int pa_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUPPA_PA_H_ */

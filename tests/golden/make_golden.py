@@ -1,0 +1,104 @@
+"""Regenerate the committed golden fixtures under tests/golden/.
+
+    python tests/golden/make_golden.py
+
+Two kinds of fixture:
+
+1. Reference outputs.  oracle/_ref/scm_ref is the reference's own sequential
+   copy model (src/PA/SPA/SerialCopyModel3.cpp, built by `make -C oracle ref`
+   from the cuPPA-Public sources).  For each (n, M, p) below it writes the
+   "Degree,Count" CSV of src/PA/SPA/PAHelper.hpp:15-67.  The reference seeds its
+   MT19937-64 with the default 5489 and its seed graph is the star seed, so these
+   runs are deterministic.  They pin the oracle's MT_REF mode exactly and are the
+   samples for the statistical comparison of the Philox generator.
+2. Oracle digests.  FNV-1a 64 of the oracle's Philox-mode edge lists (slot
+   order and canonical, int64 little-endian) for a fixed list of shapes, plus one
+   tiny full edge list.  They pin the oracle itself across edits.
+
+Needs the reference tree only for part 1 (scm_ref must already be built).
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+import _oracle as orc  # noqa: E402
+
+# (n, M, p) runs of the reference scm.  Small ones pin MT_REF exactly; the n=10^6
+# d=4 runs are the statistical samples (tail exponent, KS on degrees).
+SCM_RUNS = [
+    (100000, 4, 0.5), (20000, 4, 0.2), (20000, 4, 0.8), (10000, 4, 0.0),
+    (20000, 8, 0.5), (5000, 1, 0.5), (30000, 16, 0.3), (10000, 32, 0.5),
+    (3000, 2, 1.0), (1000000, 4, 0.2), (1000000, 4, 0.5), (1000000, 4, 0.8),
+]
+
+# Philox-mode digests: (n, d, p, seed, seed_mode).
+DIGEST_CASES = [
+    (100000, 4, 0.5, 42, orc.SEED_CLIQUE),      # the CPU-runnable benchmark configuration
+    (100000, 4, 0.5, 42, orc.SEED_STAR_REF),
+    (20000, 16, 0.5, 7, orc.SEED_CLIQUE),
+    (20000, 4, 0.0, 1234, orc.SEED_CLIQUE),
+    (20000, 4, 0.0, 1234, orc.SEED_STAR_REF),
+    (5000, 1, 0.3, 3, orc.SEED_CLIQUE),
+    (5000, 32, 0.9, 5, orc.SEED_CLIQUE),
+    (4000, 3, 1.0, 11, orc.SEED_CLIQUE),
+    (4000, 7, 0.1, 2 ** 40 + 17, orc.SEED_STAR_REF),
+]
+
+
+def scm_fixtures():
+    if not os.path.exists(orc.REF_SCM):
+        raise SystemExit(f"{orc.REF_SCM} missing: run `make -C oracle ref` first")
+    outdir = os.path.join(HERE, "scm_dd")
+    os.makedirs(outdir, exist_ok=True)
+    index = []
+    for n, m, p in SCM_RUNS:
+        name = f"scm_n{n}_m{m}_p{p}.csv"
+        with tempfile.TemporaryDirectory() as td:
+            subprocess.run([orc.REF_SCM, str(n), str(m), str(p), td, name], check=True,
+                           cwd=td, stdout=subprocess.DEVNULL)
+            with open(os.path.join(td, name)) as f:
+                text = f.read()
+        with open(os.path.join(outdir, name), "w") as f:
+            f.write(text)
+        index.append({"n": n, "m": m, "p": p, "file": f"scm_dd/{name}"})
+    with open(os.path.join(HERE, "scm_dd.json"), "w") as f:
+        json.dump({"generator": "reference -A scm (SerialCopyModel3.cpp), MT19937-64 seed 5489, "
+                                "star seed", "runs": index}, f, indent=1)
+
+
+def digest_fixtures():
+    cases = []
+    for n, d, p, seed, mode in DIGEST_CASES:
+        G, retries = orc.generate(n, d, p, seed, mode, orc.RNG_PHILOX, with_retries=True)
+        slot = orc.pairs_slot_order(G, mode)
+        can = orc.pairs_canonical(G, mode)
+        cases.append({
+            "n": n, "d": d, "p": p, "seed": seed, "seed_mode": mode,
+            "edges": int(slot.shape[0]), "retries": retries,
+            "fnv_slot_i64": f"{orc.fnv1a64(slot):016x}",
+            "fnv_canonical_i64": f"{orc.fnv1a64(can):016x}",
+            "fnv_canonical_i32": f"{orc.fnv1a64(can.astype(np.int32)):016x}",
+        })
+    with open(os.path.join(HERE, "philox_digests.json"), "w") as f:
+        json.dump({"digest": "FNV-1a 64 over little-endian (src, dst) pairs", "cases": cases},
+                  f, indent=1)
+    # one tiny full edge list in the reference's text format ("u v" per line)
+    G = orc.generate(40, 3, 0.5, 42, orc.SEED_CLIQUE)
+    can = orc.pairs_canonical(G, orc.SEED_CLIQUE)
+    with open(os.path.join(HERE, "tiny_n40_d3_p0.5_s42_clique.txt"), "w") as f:
+        f.writelines(f"{u} {v}\n" for u, v in can.tolist())
+
+
+if __name__ == "__main__":
+    scm_fixtures()
+    digest_fixtures()
+    print("fixtures written to", HERE)

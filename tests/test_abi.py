@@ -1,0 +1,96 @@
+"""The C ABI without a GPU: the library loads, exports every function that
+include/*.h declares, and its host-side checks and size arithmetic agree with
+the oracle.  No compute call is made here."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+import _oracle as orc
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(pa_\w+)\s*\([^;{]*\)\s*;", text):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_the_api():
+    names = declared_functions()
+    for must in ("pa_generate", "pa_generate_finish", "pa_edges_bytes", "pa_scratch_bytes",
+                 "pa_canonicalize", "pa_degrees", "pa_strerror", "pa_graph_create"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(pa):
+    L = ctypes.CDLL(pa.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_abi_version_and_strerror(pa):
+    assert pa.lib().pa_abi_version() == 1
+    for s in range(0, 9):
+        assert pa.strerror(s)
+    assert pa.strerror(0) == "ok"
+
+
+@pytest.mark.parametrize("n,d,mode", [(100000, 4, 1), (100000, 4, 0), (10 ** 8, 16, 1),
+                                      (2 ** 30, 4, 1), (34, 32, 0), (2, 1, 1)])
+def test_edge_count_matches_oracle(pa, n, d, mode):
+    bits = 64 if n > 2 ** 31 - 1 else 32
+    prm = pa.make_params(n, d, 0.5, id_bits=bits, seed_mode=mode)
+    assert pa.edge_count(prm) == orc.edge_count(n, d, mode)
+    eb, sb = pa.sizes(prm)
+    assert eb == orc.edge_count(n, d, mode) * 2 * bits // 8
+    assert sb >= 256
+
+
+def test_param_checks(pa):
+    def rc(**kw):
+        base = dict(n=1000, d=4, p=0.5)
+        base.update(kw)
+        prm = pa.PaParams()
+        pa.lib().pa_params_init(ctypes.byref(prm))
+        for k, v in base.items():
+            setattr(prm, k, v)
+        return pa.lib().pa_params_check(ctypes.byref(prm))
+
+    assert rc() == pa.PA_OK
+    assert rc(d=0) == pa.PA_ERR_INVALID
+    assert rc(d=33) == pa.PA_ERR_NOT_SUPPORTED
+    assert rc(n=4, d=4) == pa.PA_ERR_INVALID          # fewer than d+1 nodes
+    assert rc(n=5, d=4) == pa.PA_OK                   # the seed graph alone
+    assert rc(p=-0.1) == pa.PA_ERR_INVALID
+    assert rc(p=1.5) == pa.PA_ERR_INVALID
+    assert rc(p=float("nan")) == pa.PA_ERR_INVALID
+    assert rc(id_bits=16) == pa.PA_ERR_INVALID
+    assert rc(id_bits=32, n=2 ** 31) == pa.PA_ERR_INVALID
+    assert rc(id_bits=64, n=2 ** 31) == pa.PA_OK
+    assert rc(seed_mode=7) == pa.PA_ERR_INVALID
+    assert rc(tile_passes=3) == pa.PA_ERR_INVALID
+    assert rc(flags=1) == pa.PA_ERR_INVALID
+    assert rc(flags=pa.PA_FLAG_TEST_WITHHOLD_FIRST_TILE) == pa.PA_OK
+
+
+def test_generate_rejects_bad_buffers_without_touching_the_device(pa):
+    prm = pa.make_params(1000, 4, 0.5)
+    eb, sb = pa.sizes(prm)
+    L = pa.lib()
+    # NULL buffers
+    assert L.pa_generate(ctypes.byref(prm), None, eb, None, sb, None) == pa.PA_ERR_INVALID
+    # too-small buffers (pointers are never dereferenced on this path)
+    fake = ctypes.c_void_p(0x10000)
+    assert L.pa_generate(ctypes.byref(prm), fake, eb - 1, fake, sb, None) == pa.PA_ERR_CAPACITY
+    assert L.pa_generate(ctypes.byref(prm), fake, eb, fake, sb - 1, None) == pa.PA_ERR_CAPACITY
+    # misaligned
+    bad = ctypes.c_void_p(0x10004)
+    assert L.pa_generate(ctypes.byref(prm), bad, eb, fake, sb, None) == pa.PA_ERR_INVALID

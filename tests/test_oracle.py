@@ -1,0 +1,220 @@
+"""The CPU oracle, pinned before it is trusted.
+
+* Philox4x32-10 against the published known-answer vectors of the Random123
+  distribution (Salmon et al., SC'11);
+* MT19937-64 against the value the C++ standard fixes for the 10000th output of
+  a default-seeded std::mt19937_64 ([rand.predef]);
+* MT_REF mode (the reference's own RNG and draw order) against the degree
+  distributions written by the reference `-A scm` itself (tests/golden/scm_dd,
+  made by tests/golden/make_golden.py) -- byte-for-byte;
+* the model's hand-checkable cases (SURVEY test pyramid item 2): p = 1, p = 0,
+  seed shapes, duplicate retries, id-width boundaries;
+* the oracle's own Philox-mode digests (regression pin).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import _oracle as orc
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+# Random123 kat_vectors, philox4x32 with 10 rounds: (ctr, key, expected)
+PHILOX_KAT = [
+    ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+    ((0xFFFFFFFF,) * 4, (0xFFFFFFFF,) * 2, (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+    ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+     (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)),
+]
+
+
+@pytest.mark.parametrize("ctr,key,want", PHILOX_KAT)
+def test_philox_known_answers(ctr, key, want):
+    assert orc.philox(ctr, key) == want
+
+
+def test_mt19937_64_standard_value():
+    out = orc.mt19937_64(5489, 10000)
+    assert int(out[-1]) == 9981545732273789042
+
+
+def _scm_runs():
+    with open(os.path.join(GOLD, "scm_dd.json")) as f:
+        return json.load(f)["runs"]
+
+
+@pytest.mark.parametrize("run", [r for r in _scm_runs() if r["n"] <= 100000],
+                         ids=lambda r: f"n{r['n']}_m{r['m']}_p{r['p']}")
+def test_mt_ref_mode_reproduces_reference_scm(run):
+    """The oracle's copy-model loop, driven by the reference's RNG, gives the
+    reference's exact degree distribution: the model semantics shared with the
+    Philox mode are the reference's."""
+    G = orc.generate(run["n"], run["m"], run["p"], 5489, orc.SEED_STAR_REF, orc.RNG_MT_REF)
+    mine = orc.dd_csv_from_degrees(orc.degrees(G, orc.SEED_STAR_REF))
+    with open(os.path.join(GOLD, run["file"])) as f:
+        ref = f.read()
+    assert mine == ref
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("run", [r for r in _scm_runs() if r["n"] > 100000],
+                         ids=lambda r: f"n{r['n']}_m{r['m']}_p{r['p']}")
+def test_mt_ref_mode_reproduces_reference_scm_large(run):
+    G = orc.generate(run["n"], run["m"], run["p"], 5489, orc.SEED_STAR_REF, orc.RNG_MT_REF)
+    mine = orc.dd_csv_from_degrees(orc.degrees(G, orc.SEED_STAR_REF))
+    with open(os.path.join(GOLD, run["file"])) as f:
+        assert mine == f.read()
+
+
+@pytest.mark.parametrize("case", json.load(open(os.path.join(GOLD, "philox_digests.json")))["cases"],
+                         ids=lambda c: f"n{c['n']}_d{c['d']}_p{c['p']}_s{c['seed']}_m{c['seed_mode']}")
+def test_philox_mode_digests(case):
+    G, retries = orc.generate(case["n"], case["d"], case["p"], case["seed"], case["seed_mode"],
+                              orc.RNG_PHILOX, with_retries=True)
+    slot = orc.pairs_slot_order(G, case["seed_mode"])
+    can = orc.pairs_canonical(G, case["seed_mode"])
+    assert slot.shape[0] == case["edges"]
+    assert retries == case["retries"]
+    assert f"{orc.fnv1a64(slot):016x}" == case["fnv_slot_i64"]
+    assert f"{orc.fnv1a64(can):016x}" == case["fnv_canonical_i64"]
+    assert f"{orc.fnv1a64(can.astype(np.int32)):016x}" == case["fnv_canonical_i32"]
+
+
+def test_tiny_text_fixture():
+    G = orc.generate(40, 3, 0.5, 42, orc.SEED_CLIQUE)
+    can = orc.pairs_canonical(G, orc.SEED_CLIQUE)
+    text = "".join(f"{u} {v}\n" for u, v in can.tolist())
+    with open(os.path.join(GOLD, "tiny_n40_d3_p0.5_s42_clique.txt")) as f:
+        assert text == f.read()
+
+
+# ---- model properties -------------------------------------------------------
+
+def _check_simple_graph(G, d, seed_mode):
+    n = G.shape[0]
+    gen = G[d + 1:]
+    u = np.arange(d + 1, n)[:, None]
+    assert (gen >= 0).all() and (gen < u).all(), "targets in [0, u)"
+    s = np.sort(gen, axis=1)
+    assert (np.diff(s, axis=1) > 0).all(), "no multi-edges within a node"
+    can = orc.pairs_canonical(G, seed_mode)
+    assert (can[:, 0] > can[:, 1]).all(), "no self loops; u > v"
+    key = can[:, 0] * n + can[:, 1]
+    assert (np.diff(key) > 0).all(), "canonical list strictly sorted"
+
+
+@pytest.mark.parametrize("d", [1, 2, 3, 4, 8, 16, 32])
+@pytest.mark.parametrize("p", [0.0, 0.1, 0.5, 0.9, 1.0])
+@pytest.mark.parametrize("mode", [orc.SEED_STAR_REF, orc.SEED_CLIQUE])
+def test_simple_graph_properties(d, p, mode):
+    n = 3000
+    G = orc.generate(n, d, p, 1000 + d, mode)
+    _check_simple_graph(G, d, mode)
+    assert orc.pairs_slot_order(G, mode).shape[0] == orc.edge_count(n, d, mode)
+
+
+def test_seed_shapes():
+    d = 5
+    G = orc.generate(d + 1, d, 0.5, 1, orc.SEED_CLIQUE)
+    can = orc.pairs_canonical(G, orc.SEED_CLIQUE)
+    want = [(v, w) for v in range(d + 1) for w in range(v)]
+    assert [tuple(x) for x in can.tolist()] == want
+    G = orc.generate(d + 1, d, 0.5, 1, orc.SEED_STAR_REF)
+    assert G[:d].tolist() == [[i] * d for i in range(d)]
+    assert G[d].tolist() == list(range(d))
+    can = orc.pairs_canonical(G, orc.SEED_STAR_REF)
+    assert [tuple(x) for x in can.tolist()] == [(d, j) for j in range(d)]
+    assert orc.seed_edge_count(d, orc.SEED_CLIQUE) == 15
+    assert orc.seed_edge_count(d, orc.SEED_STAR_REF) == 5
+
+
+def test_p0_star_ref_is_complete_bipartite():
+    """p = 0 with the reference seed: every node copies a seed target, so every
+    new node links to exactly {0..d-1} -- K_{d,n-d}, no power law."""
+    n, d = 5000, 4
+    G = orc.generate(n, d, 0.0, 99, orc.SEED_STAR_REF)
+    assert (np.sort(G[d + 1:], axis=1) == np.arange(d)).all()
+
+
+def test_p0_clique_closure():
+    n, d = 5000, 4
+    G = orc.generate(n, d, 0.0, 99, orc.SEED_CLIQUE)
+    assert G[d + 1:].max() <= d
+
+
+def test_p1_uniform_distinct():
+    """p = 1: direct picks only, so every slot is a uniform earlier node."""
+    n, d = 200000, 4
+    G = orc.generate(n, d, 1.0, 5, orc.SEED_CLIQUE)
+    u = np.arange(d + 1, n)
+    frac = G[d + 1:, 0] / u   # first slot never retries: uniform on [0, 1)
+    hist, _ = np.histogram(frac, bins=10, range=(0, 1))
+    expect = len(frac) / 10
+    assert (np.abs(hist - expect) < 5 * np.sqrt(expect)).all()
+
+
+def test_duplicate_retry_path():
+    """Retries happen and the accepted draw is the first non-duplicate: replay
+    node u slot by slot with the raw Philox draws."""
+    n, d, p, seed = 300, 8, 0.0, 77
+    G, retries = orc.generate(n, d, p, seed, orc.SEED_CLIQUE, with_retries=True)
+    assert retries > 0
+    pth = orc.p_threshold(p)
+    replay_retries = 0
+    for u in range(d + 1, n):
+        row = []
+        for i in range(d):
+            r = 0
+            while True:
+                w = orc.philox((u & 0xFFFFFFFF, u >> 32, i, r), (seed & 0xFFFFFFFF, seed >> 32))
+                v = ((((w[1] << 32) | w[0]) * u) >> 64)
+                k = (w[3] * d) >> 32
+                cand = v if w[2] < pth else int(G[v, k])
+                if cand not in row:
+                    row.append(cand)
+                    break
+                r += 1
+                replay_retries += 1
+        assert row == G[u].tolist()
+    assert replay_retries == retries
+
+
+def test_p_threshold():
+    assert orc.p_threshold(0.0) == 0
+    assert orc.p_threshold(1.0) == 1 << 32
+    assert orc.p_threshold(0.5) == 1 << 31
+    assert orc.p_threshold(0.25) == 1 << 30
+
+
+def test_id_width_boundaries():
+    """Large node ids: the Philox counter carries u's high word, and the
+    multiply-shift keeps v < u.  A tiny graph cannot reach 2^32 nodes, so check
+    the draw arithmetic directly at the boundary."""
+    for u in (2 ** 31 - 1, 2 ** 31, 2 ** 32 - 1, 2 ** 32, 2 ** 33 + 5):
+        for i in range(4):
+            w = orc.philox((u & 0xFFFFFFFF, u >> 32, i, 0), (7, 0))
+            v = ((((w[1] << 32) | w[0]) * u) >> 64)
+            assert 0 <= v < u
+    # the counter's high word matters
+    a = orc.philox((5, 0, 0, 0), (1, 2))
+    b = orc.philox((5, 1, 0, 0), (1, 2))
+    assert a != b
+
+
+def test_csr_sorted_and_symmetric():
+    n, d = 4000, 4
+    for mode in (orc.SEED_STAR_REF, orc.SEED_CLIQUE):
+        G = orc.generate(n, d, 0.3, 3, mode)
+        rowptr, col = orc.csr(G, mode)
+        deg = orc.degrees(G, mode)
+        assert (np.diff(rowptr) == deg).all()
+        for x in range(n):
+            row = col[rowptr[x]:rowptr[x + 1]]
+            assert (np.diff(row) > 0).all()
+        can = orc.pairs_canonical(G, mode)
+        und = np.concatenate([can, can[:, ::-1]])
+        order = np.lexsort((und[:, 1], und[:, 0]))
+        assert (und[order, 1] == col).all()

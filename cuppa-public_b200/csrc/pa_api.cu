@@ -37,7 +37,7 @@ int make_plan(const pa_params *prm, GenPlan *plan)
     GenPlan p{};
     p.id_bytes = prm->id_bits / 8;
     p.groups = 32u / prm->d;
-    p.passes = prm->tile_passes ? prm->tile_passes : 4u;
+    p.passes = prm->tile_passes ? prm->tile_passes : 2u;
     p.tile_nodes = p.groups * p.passes;
     p.u_first = (uint64_t)prm->d + 1;
     const uint64_t n_gen = prm->n - p.u_first;
@@ -46,7 +46,10 @@ int make_plan(const pa_params *prm, GenPlan *plan)
     p.n_edges = p.seed_edges + n_gen * prm->d;
     p.pth = p_threshold(prm->p);
     p.edges_bytes = p.n_edges * 2ull * p.id_bytes;
-    p.scratch_bytes = kCtlBytes + ((p.n_tiles * 4ull + 255ull) & ~255ull);
+    p.n_sb = (p.n_tiles + kSbTiles - 1) / kSbTiles;
+    p.sb_offset = kCtlBytes + ((p.n_tiles * 4ull + 255ull) & ~255ull);
+    p.trace_offset = p.sb_offset + ((p.n_sb * 4ull + 255ull) & ~255ull);
+    p.scratch_bytes = p.trace_offset + (uint64_t)kTraceMax * 16ull;
     p.spin_limit_ns = prm->spin_limit_ns ? prm->spin_limit_ns : 2000000000ull;
     *plan = p;
     return PA_OK;
@@ -168,10 +171,36 @@ int pa_generate_finish(const void *d_scratch, pa_stats *out, void *stream)
         out->retries = ctl.retries;
         out->waits = ctl.waits;
         out->tiles = ctl.tiles;
+        out->pending_reads = ctl.pending_reads;
+        out->pending_polls = ctl.pending_polls;
         out->status = ctl.error;
         out->reserved = 0;
     }
     return (int)ctl.error;
+}
+
+int pa_generate_trace(const pa_params *prm, const void *d_scratch, uint64_t *out, uint32_t max_samples,
+                      uint32_t *count, void *stream)
+{
+    GenPlan p;
+    const int rc = make_plan(prm, &p);
+    if (rc != PA_OK) return rc;
+    if (!d_scratch || !count || (max_samples && !out)) return PA_ERR_INVALID;
+    GenCtl ctl;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemcpyAsync(&ctl, d_scratch, sizeof(ctl), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    uint32_t n = ctl.trace_count < kTraceMax ? ctl.trace_count : kTraceMax;
+    if (n > max_samples) n = max_samples;
+    if (n) {
+        e = cudaMemcpyAsync(out, (const unsigned char *)d_scratch + p.trace_offset, n * 16ull,
+                            cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return set_cuda_error(e);
+    }
+    *count = n;
+    return PA_OK;
 }
 
 int pa_graph_create(const pa_params *prm, pa_graph *g)

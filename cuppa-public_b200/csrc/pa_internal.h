@@ -9,21 +9,38 @@
 namespace pa {
 
 // Control block at the head of the generation scratch.  Cleared before every
-// launch; the kernel's tile ticket, completion watermark, counters and device
-// status live here.
+// launch.  The tile ticket (the hottest atomic) has a 128-byte line of its own;
+// the watermark, the device status and the counters share the next one.
 struct GenCtl {
-    unsigned long long ticket;   // next tile to claim
-    unsigned long long water;    // tiles [0, water) are complete and visible
+    unsigned long long ticket;   // next chunk of tiles to claim
+    unsigned long long pad0[15];
+    unsigned long long water;    // superblocks [0, water) are complete and visible
     unsigned long long retries;  // rejected draws
     unsigned long long waits;    // resolve iterations that made no progress
     unsigned long long tiles;    // tiles completed
+    unsigned long long pending_reads;  // copy reads whose source tile was not yet known complete
+    unsigned long long pending_polls;  // flag polls that found the source tile unfinished
     uint32_t error;              // pa_status raised on the device
-    uint32_t pad;
-    unsigned long long reserved[2];
+    uint32_t trace_count;        // progress samples written
+    unsigned long long t_start;  // globaltimer at the watermark warp's start
 };
-static_assert(sizeof(GenCtl) == 64, "GenCtl layout");
+static_assert(sizeof(GenCtl) == 192, "GenCtl layout");
 
-constexpr uint64_t kCtlBytes = 256;  // flags start 256 B into the scratch
+// Read-mostly copies of the watermark and the device status, one 128-byte line
+// each; a warp reads copy (warp id mod kReps), so waiting warps spread their
+// polls over kReps L2 lines instead of one.
+struct GenRep {
+    unsigned long long water;
+    uint32_t error;
+    uint32_t pad[29];
+};
+static_assert(sizeof(GenRep) == 128, "GenRep layout");
+constexpr uint32_t kReps = 16;
+constexpr uint64_t kRepOffset = 256;                        // replicas after GenCtl
+constexpr uint64_t kCtlBytes = kRepOffset + kReps * 128;    // flags start here
+constexpr uint32_t kSbTiles = 64;    // tiles per superblock (watermark granularity)
+constexpr uint32_t kClaimTiles = 4;  // consecutive tiles claimed by one ticket
+constexpr uint32_t kTraceMax = 2048; // progress samples kept per generation
 
 // Resolved launch geometry of one generation.
 struct GenPlan {
@@ -33,6 +50,9 @@ struct GenPlan {
     uint32_t tile_nodes;    // groups * passes
     uint64_t u_first;       // d + 1
     uint64_t n_tiles;
+    uint64_t n_sb;          // superblocks of kSbTiles tiles
+    uint64_t sb_offset;     // byte offset of the superblock counters in the scratch
+    uint64_t trace_offset;  // byte offset of the progress trace in the scratch
     uint64_t seed_edges;
     uint64_t n_edges;
     uint64_t pth;           // direct threshold

@@ -77,6 +77,8 @@ class PaStats(ctypes.Structure):
         ("retries", ctypes.c_uint64),
         ("waits", ctypes.c_uint64),
         ("tiles", ctypes.c_uint64),
+        ("pending_reads", ctypes.c_uint64),
+        ("pending_polls", ctypes.c_uint64),
         ("status", ctypes.c_uint32),
         ("reserved", ctypes.c_uint32),
     ]
@@ -112,6 +114,8 @@ _SIGS = {
     "pa_generate": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_uint64,
                                    ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),
     "pa_generate_finish": (ctypes.c_int, [ctypes.c_void_p, _P(PaStats), ctypes.c_void_p]),
+    "pa_generate_trace": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_uint32, _P(ctypes.c_uint32), ctypes.c_void_p]),
     "pa_canonicalize": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_void_p,
                                        ctypes.c_void_p]),
     "pa_degrees": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_void_p,
@@ -212,6 +216,19 @@ def finish(scratch, stream=None) -> PaStats:
     lib().pa_generate_finish(ctypes.c_void_p(scratch.data_ptr()), ctypes.byref(st),
                              ctypes.c_void_p(_stream_ptr(stream)))
     return st
+
+
+def trace(prm: PaParams, scratch, stream=None, max_samples: int = 2048):
+    """Progress samples of the last generation into `scratch`: list of
+    (elapsed ns, nodes complete)."""
+    import numpy as np
+    buf = np.zeros(2 * max_samples, dtype=np.uint64)
+    cnt = ctypes.c_uint32()
+    check(lib().pa_generate_trace(ctypes.byref(prm), ctypes.c_void_p(scratch.data_ptr()),
+                                  buf.ctypes.data_as(ctypes.c_void_p), max_samples,
+                                  ctypes.byref(cnt), ctypes.c_void_p(_stream_ptr(stream))),
+          "pa_generate_trace")
+    return [(int(buf[2 * i]), int(buf[2 * i + 1])) for i in range(cnt.value)]
 
 
 def generate(prm: PaParams, stream=None, raise_on_error: bool = True):

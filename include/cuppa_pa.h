@@ -80,6 +80,8 @@ typedef struct pa_stats {
     uint64_t retries;       /* draws rejected as duplicates                               */
     uint64_t waits;         /* resolve iterations that waited on an unfinished tile       */
     uint64_t tiles;         /* tiles completed                                            */
+    uint64_t pending_reads; /* copy reads whose source tile was not yet known complete    */
+    uint64_t pending_polls; /* completion-flag polls that found the source tile unfinished */
     uint32_t status;        /* pa_status seen on the device (PA_OK or PA_ERR_SPIN_TIMEOUT) */
     uint32_t reserved;
 } pa_stats;
@@ -105,6 +107,14 @@ int pa_generate(const pa_params *prm, void *d_edges, uint64_t edges_bytes, void 
 /* Wait for the stream, then copy the status and counters of the generation that
  * last used d_scratch.  Returns the device status. */
 int pa_generate_finish(const void *d_scratch, pa_stats *out, void *stream);
+
+/* Progress trace of the generation that last used d_scratch (waits for the
+ * stream): up to max_samples pairs (elapsed ns since the launch's first warp
+ * started, nodes known complete), 2 x uint64 each, in time order; *count gets
+ * the number written.  The device side of the per-stage timing table the
+ * reference writes (src/PA/cuPPA/cuPPA_1.cu:84-87,217-223). */
+int pa_generate_trace(const pa_params *prm, const void *d_scratch, uint64_t *out,
+                      uint32_t max_samples, uint32_t *count, void *stream);
 
 /* ---- post-processing ------------------------------------------------------ */
 /* Sort every node's d pairs by dst in place (or into d_out): the canonical edge

@@ -1,0 +1,93 @@
+"""Statistical agreement with the reference's own generator.
+
+The reference GPU path draws from time-seeded curand (src/PA/cuPPA/cuPPA_1.cu:39)
+and its CPU path from MT19937-64, so no Philox stream can match either
+bit-for-bit.  The model is the same, so degree distributions must agree: the
+reference `-A scm` runs for n = 10^6, M = 4 (tests/golden/scm_dd, written by the
+reference binary) are compared with the Philox generator at the same n, d, p and
+the reference's seed graph, by
+
+* the two-sample Kolmogorov-Smirnov statistic on the degree distributions,
+  bound 1.949 * sqrt(2 / 10^6) = 0.00276 (the critical value at alpha = 0.001);
+* the tail exponent MLE  alpha = 1 + N / sum(ln(k / (k_min - 1/2))),  k_min = 8,
+  within 0.02 of the reference's.
+
+At p = 0 the model is degenerate (K_{d, n-d} with the reference seed: every new
+node links to exactly 0..d-1), so there the distributions must be identical.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import _oracle as orc
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+KS_BOUND = 1.949 * np.sqrt(2 / 1e6)
+ALPHA_TOL = 0.02
+
+
+def _hist(text):
+    h = orc.hist_from_dd_csv(text)
+    ks = np.array(sorted(h))
+    return ks, np.array([h[k] for k in ks])
+
+
+def ks_statistic(h1, h2):
+    k = np.union1d(h1[0], h2[0])
+
+    def cdf(h):
+        c = np.zeros(len(k))
+        c[np.searchsorted(k, h[0])] = h[1]
+        return np.cumsum(c) / c.sum()
+
+    return float(np.abs(cdf(h1) - cdf(h2)).max())
+
+
+def tail_alpha(h, kmin=8):
+    m = h[0] >= kmin
+    k, c = h[0][m], h[1][m]
+    return float(1 + c.sum() / np.sum(c * np.log(k / (kmin - 0.5))))
+
+
+def _ref(p):
+    with open(os.path.join(GOLD, "scm_dd", f"scm_n1000000_m4_p{p}.csv")) as f:
+        return _hist(f.read())
+
+
+@pytest.mark.parametrize("p", [0.2, 0.5, 0.8])
+def test_oracle_matches_reference_distribution(p):
+    G = orc.generate(10 ** 6, 4, p, 1, orc.SEED_STAR_REF)
+    mine = _hist(orc.dd_csv_from_degrees(orc.degrees(G, orc.SEED_STAR_REF)))
+    ref = _ref(p)
+    assert ks_statistic(mine, ref) < KS_BOUND
+    assert abs(tail_alpha(mine) - tail_alpha(ref)) < ALPHA_TOL
+
+
+def test_p0_degenerate_matches_reference_exactly():
+    with open(os.path.join(GOLD, "scm_dd", "scm_n10000_m4_p0.0.csv")) as f:
+        ref = f.read()
+    G = orc.generate(10000, 4, 0.0, 7, orc.SEED_STAR_REF)
+    assert orc.dd_csv_from_degrees(orc.degrees(G, orc.SEED_STAR_REF)) == ref
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("p", [0.2, 0.5, 0.8])
+def test_gpu_generator_matches_reference_distribution(pa, cuda_ok, p):
+    prm = pa.make_params(10 ** 6, 4, p, seed=99, id_bits=32, seed_mode=pa.PA_SEED_STAR_REF)
+    edges, st = pa.generate(prm)
+    csv = pa.degree_distribution_csv(pa.degrees(prm, edges))
+    mine, ref = _hist(csv), _ref(p)
+    assert ks_statistic(mine, ref) < KS_BOUND
+    assert abs(tail_alpha(mine) - tail_alpha(ref)) < ALPHA_TOL
+
+
+@pytest.mark.gpu
+def test_gpu_clique_seed_p0_closure(pa, cuda_ok):
+    """Benchmark configuration's p = 0 run: with the (d+1)-clique seed every
+    target stays in {0..d} -- the structure the degree check can see."""
+    prm = pa.make_params(200_000, 4, 0.0, seed=1234, id_bits=64, seed_mode=pa.PA_SEED_CLIQUE)
+    edges, st = pa.generate(prm)
+    assert int(edges[:, 1].max()) <= 4
+    deg = pa.degrees(prm, edges).cpu().numpy()
+    assert (deg[5:] == 4).all()

@@ -108,6 +108,24 @@ int pa_generate(const pa_params *prm, void *d_edges, uint64_t edges_bytes, void 
  * last used d_scratch.  Returns the device status. */
 int pa_generate_finish(const void *d_scratch, pa_stats *out, void *stream);
 
+/* Generation for callers that cannot allocate device memory (a host whose
+ * memory pool forbids further allocations, or a latency-critical request loop
+ * that must not stall in cudaMalloc/cudaFree).  No counterpart in the
+ * reference.  The scratch lives in a PA_NOALLOC_SCRATCH_BYTES (16 MiB)
+ * __device__ array inside this library, held on every GPU that loads it until
+ * the process exits; the caller passes only the parameters and the edge
+ * buffer.  Requests whose scratch exceeds the array (roughly n > 65 million
+ * nodes at d = 4, n > 8 million at d = 32) return PA_ERR_CAPACITY before any GPU
+ * work.  The first call on a device looks the array's address up with
+ * cudaGetSymbolAddress (with that device current) and caches it: make that
+ * first call before any stream capture begins.  All calls on a device share the
+ * array, so calls whose GPU work overlaps race on it: issue them on one stream
+ * or serialize them.  Each call clears what it uses, generates on `stream`,
+ * waits for it, fills *stats (may be NULL) and returns the device status. */
+#define PA_NOALLOC_SCRATCH_BYTES (16u << 20)
+int pa_generate_noalloc(const pa_params *prm, void *d_edges, uint64_t edges_bytes,
+                        pa_stats *stats, void *stream);
+
 /* Progress trace of the generation that last used d_scratch (waits for the
  * stream): up to max_samples pairs (elapsed ns since the launch's first warp
  * started, nodes known complete), 2 x uint64 each, in time order; *count gets

@@ -55,6 +55,9 @@ WORKLOADS = {
     "c3s": dict(n=2 ** 25, d=4, p=0.5, seed=1234, id_bits=64, seed_mode=CLIQUE,
                 name="copy-model PA, n=2^25, d=4, p=0.5, int64 ids, clique seed, Philox seed 1234 "
                      "(profiling size)"),
+    "c3m": dict(n=2 ** 26, d=4, p=0.5, seed=1234, id_bits=64, seed_mode=CLIQUE,
+                name="copy-model PA, n=2^26, d=4, p=0.5, int64 ids, clique seed, Philox seed 1234 "
+                     "(traffic capture size)"),
     "c1": dict(n=10 ** 5, d=4, p=0.5, seed=42, id_bits=32, seed_mode=CLIQUE,
                name="copy-model PA, n=10^5, d=4, p=0.5, int32 ids, clique seed, Philox seed 42"),
 }

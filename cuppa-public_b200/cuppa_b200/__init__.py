@@ -43,6 +43,8 @@ PA_ERR_NOT_FOUND = 8
 PA_SEED_STAR_REF = 0
 PA_SEED_CLIQUE = 1
 PA_LAYOUT_PAIRS = 0
+PA_FORMAT_TEXT = 0
+PA_FORMAT_BINARY = 1
 
 # Test-only: the generator never publishes its first tile, so every wait on it
 # runs into the wait limit (a flag that nothing sets).
@@ -120,6 +122,15 @@ _SIGS = {
                                        ctypes.c_void_p]),
     "pa_degrees": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_void_p,
                                   ctypes.c_void_p]),
+    "pa_csr_bytes": (ctypes.c_int, [_P(PaParams), _P(ctypes.c_uint64), _P(ctypes.c_uint64),
+                                    _P(ctypes.c_uint64)]),
+    "pa_build_csr": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                    ctypes.c_void_p]),
+    "pa_write_edges": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_char_p,
+                                      ctypes.c_int, ctypes.c_void_p]),
+    "pa_write_degree_distribution": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p,
+                                                    ctypes.c_char_p, ctypes.c_void_p]),
     "pa_graph_create": (ctypes.c_int, [_P(PaParams), _P(PaGraph)]),
     "pa_graph_generate": (ctypes.c_int, [_P(PaGraph), ctypes.c_void_p, _P(PaStats)]),
     "pa_graph_destroy": (ctypes.c_int, [_P(PaGraph)]),
@@ -258,6 +269,37 @@ def degrees(prm: PaParams, edges, stream=None):
     return deg
 
 
+def build_csr(prm: PaParams, edges, stream=None):
+    """Undirected CSR (rowptr int64[n+1], col ids[2E]) with sorted rows."""
+    torch = _torch()
+    rb, cb, sb = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+    check(lib().pa_csr_bytes(ctypes.byref(prm), ctypes.byref(rb), ctypes.byref(cb),
+                             ctypes.byref(sb)), "pa_csr_bytes")
+    rowptr = torch.empty(prm.n + 1, dtype=torch.int64, device=edges.device)
+    dt = torch.int64 if prm.id_bits == 64 else torch.int32
+    col = torch.empty(max(cb.value // (prm.id_bits // 8), 1), dtype=dt, device=edges.device)
+    scratch = torch.empty(sb.value, dtype=torch.uint8, device=edges.device)
+    check(lib().pa_build_csr(ctypes.byref(prm), ctypes.c_void_p(edges.data_ptr()),
+                             ctypes.c_void_p(rowptr.data_ptr()), ctypes.c_void_p(col.data_ptr()),
+                             ctypes.c_void_p(scratch.data_ptr()), sb.value,
+                             ctypes.c_void_p(_stream_ptr(stream))), "pa_build_csr")
+    return rowptr, col[: cb.value // (prm.id_bits // 8)]
+
+
+def write_edges(prm: PaParams, edges, path: str, binary: bool = False, stream=None) -> None:
+    """PAHelper::writeGraphToDisk's "u v" text (or raw pairs) from the device."""
+    check(lib().pa_write_edges(ctypes.byref(prm), ctypes.c_void_p(edges.data_ptr()),
+                               path.encode(), PA_FORMAT_BINARY if binary else PA_FORMAT_TEXT,
+                               ctypes.c_void_p(_stream_ptr(stream))), "pa_write_edges")
+
+
+def write_degree_distribution(prm: PaParams, edges, path: str, stream=None) -> None:
+    """cuPPA::printDegreeDistribution's "Degree,Count" CSV, computed on the device."""
+    check(lib().pa_write_degree_distribution(ctypes.byref(prm), ctypes.c_void_p(edges.data_ptr()),
+                                             path.encode(), ctypes.c_void_p(_stream_ptr(stream))),
+          "pa_write_degree_distribution")
+
+
 def degree_distribution_csv(deg) -> str:
     """'Degree,Count' CSV of src/PA/cuPPA/cuPPA.cu:150-157 (degree-0 nodes skipped)."""
     torch = _torch()
@@ -325,8 +367,7 @@ class cuPPA:  # noqa: N801 - reference class name
         outputDir/distfile1."""
         if self.edges is None:
             raise RuntimeError("generateGraph first")
-        csv = degree_distribution_csv(degrees(self._prm, self.edges))
         path = os.path.join(conf._outputDir, conf._distfile1)
-        with open(path, "w") as f:
-            f.write(csv)
-        return csv
+        write_degree_distribution(self._prm, self.edges, path)
+        with open(path) as f:
+            return f.read()

@@ -141,6 +141,34 @@ int pa_canonicalize(const pa_params *prm, const void *d_edges, void *d_out, void
 /* Undirected degree of every node: d_deg is int64[n]. */
 int pa_degrees(const pa_params *prm, const void *d_edges, int64_t *d_deg, void *stream);
 
+/* ---- CSR ------------------------------------------------------------------ */
+/* Undirected CSR of a generated edge list (PAIRS layout, slot or canonical
+ * order): every edge appears in both rows, and every row is sorted ascending.
+ * d_rowptr is int64[n+1]; d_col holds 2 * pa_edge_count() ids of id_bits width.
+ * Sizes of the three buffers: */
+int pa_csr_bytes(const pa_params *prm, uint64_t *rowptr_bytes, uint64_t *col_bytes,
+                 uint64_t *scratch_bytes);
+/* Builds the CSR on `stream` and waits for it (it reads back the list of hub
+ * rows, those with more than 8192 in-neighbours, and sorts each of them with a
+ * bitmap pass over the node range). */
+int pa_build_csr(const pa_params *prm, const void *d_edges, int64_t *d_rowptr, void *d_col,
+                 void *d_scratch, uint64_t scratch_bytes, void *stream);
+
+/* ---- files ------------------------------------------------------------------ */
+enum { PA_FORMAT_TEXT = 0, PA_FORMAT_BINARY = 1 };
+/* Write the device edge list to `path`: TEXT = one "u v" line per pair, the
+ * format of PAHelper::writeGraphToDisk (src/PA/SPA/PAHelper.hpp:163-177; with
+ * PA_SEED_STAR_REF also its row order); BINARY = raw little-endian id pairs.
+ * Streams through pinned host buffers the call allocates and frees; waits. */
+int pa_write_edges(const pa_params *prm, const void *d_edges, const char *path, int format,
+                   void *stream);
+/* Write the "Degree,Count" CSV of cuPPA::printDegreeDistribution
+ * (src/PA/cuPPA/cuPPA.cu:103-165) for the graph in d_edges; degrees and their
+ * histogram are computed on the device (temporaries allocated and freed with
+ * cudaMallocAsync/cudaFreeAsync on `stream`); waits. */
+int pa_write_degree_distribution(const pa_params *prm, const void *d_edges, const char *path,
+                                 void *stream);
+
 /* ---- convenience handle (library-owned memory) ----------------------------- */
 typedef struct pa_graph {
     pa_params params;

@@ -49,7 +49,8 @@ int make_plan(const pa_params *prm, GenPlan *plan)
     p.n_sb = (p.n_tiles + kSbTiles - 1) / kSbTiles;
     p.sb_offset = kCtlBytes + ((p.n_tiles * 4ull + 255ull) & ~255ull);
     p.trace_offset = p.sb_offset + ((p.n_sb * 4ull + 255ull) & ~255ull);
-    p.scratch_bytes = p.trace_offset + (uint64_t)kTraceMax * 16ull;
+    p.level_offset = p.trace_offset + (uint64_t)kTraceMax * 16ull;
+    p.scratch_bytes = p.level_offset + kLevelAreaBytes;
     p.spin_limit_ns = prm->spin_limit_ns ? prm->spin_limit_ns : 2000000000ull;
     *plan = p;
     return PA_OK;

@@ -5,18 +5,21 @@
 //
 // Row x is [x's own targets, all < x, ascending] ++ [x's in-neighbours, all > x,
 // ascending], so it comes out sorted when both parts are:
-//   1. degrees (warp-aggregated atomics, pa_degrees' kernel);
-//   2. rowptr = exclusive scan of the degrees: a single-pass scan with decoupled
-//      look-back (tiles take ids in launch order from an atomic counter, publish
-//      their aggregate, then their inclusive prefix);
+//   1. in-degrees: one warp-aggregated atomic per pair on its destination; the
+//      value the atomic returns is the pair's rank in the destination's in part,
+//      kept (4 bytes per pair) so that step 4 needs no atomics;
+//   2. rowptr = exclusive scan of out-degree + in-degree: a single-pass scan with
+//      decoupled look-back (tiles take ids in launch order from an atomic counter,
+//      publish their aggregate, then their inclusive prefix);
 //   3. out part: each generated row's d targets ranked in registers and stored;
 //      the seed rows' targets come from the (canonical) seed edges;
-//   4. in part: every pair (u, v) appends u to v's in part through an atomic
-//      cursor (order arbitrary) ...
+//   4. in part: every pair (u, v) stores u at its rank in v's in part (order
+//      arbitrary across warps) ...
 //   5. ... then every in part is sorted: a warp per part of <= 32 entries (rank
-//      by counting; entries of a part are distinct), a CTA per part of <= 8192
-//      entries (bitonic sort in shared memory), and the few larger hub parts by
-//      a bitmap over the node range (set, then compact in order).
+//      by counting; entries of a part are distinct), a warp bitonic network in
+//      registers for <= 256 entries, a CTA bitonic sort in shared memory for
+//      <= 8192, and the few larger hub parts by a bitmap over the node range
+//      (set, then compact in order).
 #include <type_traits>
 #include <vector>
 
@@ -188,11 +191,43 @@ __global__ void out_part_kernel(const Id *E, const int64_t *rowptr, Id *col, uin
 }
 
 // ---------------------------------------------------------------------------
-// In parts: append u to v's in part.
+// In-degrees and in-part ranks.
+// ---------------------------------------------------------------------------
+template <typename Id>
+__global__ void in_degree_kernel(const Id *E, uint64_t n_edges, uint64_t n, uint32_t *cnt,
+                                 uint32_t *rank)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n_edges; base += stride) {
+        const uint64_t e = base + threadIdx.x;
+        unsigned long long v = e < n_edges ? (unsigned long long)E[2 * e + 1] : ~0ull;
+        const bool act = v < n;   // ids are used as addresses: never trust them
+        if (!act) v = ~0ull - lane;
+        const uint32_t peers = __match_any_sync(kFull, v);
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t old = 0;
+        if (act && lane == leader) old = atomicAdd(cnt + v, (uint32_t)__popc(peers));
+        old = __shfl_sync(kFull, old, leader);
+        if (act) rank[e] = old + __popc(peers & lanemask_lt());
+    }
+}
+
+// deg[x] = out-degree(x) + in-degree(x); deg[n] = 0 (so rowptr[n] is the total).
+__global__ void deg_fill_kernel(const uint32_t *cnt, const uint32_t *seed_out, uint64_t n,
+                                uint32_t d, int64_t *deg)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x <= n; x += stride)
+        deg[x] = x == n ? 0 : (int64_t)cnt[x] + (x <= d ? seed_out[x] : d);
+}
+
+// ---------------------------------------------------------------------------
+// In parts: store u at its rank in v's in part (no atomics).
 // ---------------------------------------------------------------------------
 template <typename Id>
 __global__ void in_part_kernel(const Id *E, uint64_t n_edges, uint64_t n, uint32_t d,
-                               uint64_t seed_edges, const int64_t *rowptr, uint32_t *cursor,
+                               const int64_t *rowptr, const uint32_t *rank,
                                const uint32_t *seed_out, Id *col, uint64_t col_len)
 {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -200,8 +235,7 @@ __global__ void in_part_kernel(const Id *E, uint64_t n_edges, uint64_t n, uint32
         const uint64_t u = (uint64_t)E[2 * e], v = (uint64_t)E[2 * e + 1];
         if (u >= n || v >= n) continue;   // never trust ids used as addresses
         const uint64_t outdeg = v <= d ? seed_out[v] : d;
-        const uint32_t k = atomicAdd(cursor + v, 1u);
-        const uint64_t pos = (uint64_t)rowptr[v] + outdeg + k;
+        const uint64_t pos = (uint64_t)rowptr[v] + outdeg + rank[e];
         if (pos < (uint64_t)rowptr[v + 1] && pos < col_len) col[pos] = (Id)u;
     }
 }
@@ -267,8 +301,91 @@ __global__ void sort_small_kernel(uint64_t n, uint32_t d, const int64_t *rowptr,
     }
 }
 
-// Mid parts (33..8192 entries): a CTA tests 512 rows at a time, queues the mid
-// ones in shared memory and bitonic-sorts each in shared memory.
+// Bitonic sort of N = 32*EL values held by a warp, element i = j*32 + lane in
+// v[j]; ascending.  Partners at distance s < 32 are in other lanes (shuffle),
+// at s >= 32 in the same lane.
+template <typename Id, int EL>
+__device__ __forceinline__ void warp_bitonic(Id (&v)[EL], uint32_t lane)
+{
+    constexpr uint32_t N = 32u * EL;
+#pragma unroll
+    for (uint32_t k = 2; k <= N; k <<= 1) {
+#pragma unroll
+        for (uint32_t s = k >> 1; s > 0; s >>= 1) {
+            if (s >= 32) {
+                const uint32_t js = s >> 5;
+#pragma unroll
+                for (uint32_t j = 0; j < (uint32_t)EL; ++j) {
+                    const uint32_t jp = j ^ js;
+                    if (jp > j) {
+                        const uint32_t i = j * 32 + lane;
+                        const bool up = (i & k) == 0;
+                        const Id a = v[j], b = v[jp];
+                        if ((a > b) == up) {
+                            v[j] = b;
+                            v[jp] = a;
+                        }
+                    }
+                }
+            } else {
+#pragma unroll
+                for (uint32_t j = 0; j < (uint32_t)EL; ++j) {
+                    const uint32_t i = j * 32 + lane;
+                    const Id o = __shfl_xor_sync(kFull, v[j], s);
+                    const bool up = (i & k) == 0;
+                    const bool lower = (i & s) == 0;   // i < partner
+                    v[j] = (lower == up) ? (v[j] < o ? v[j] : o) : (v[j] > o ? v[j] : o);
+                }
+            }
+        }
+    }
+}
+
+template <typename Id, int EL>
+__device__ __forceinline__ void warp_sort_part(Id *col, uint64_t b, uint32_t len, uint32_t lane)
+{
+    const Id pad = (Id)(~(typename std::make_unsigned<Id>::type)0 >> 1);
+    Id v[EL];
+#pragma unroll
+    for (int j = 0; j < EL; ++j) {
+        const uint32_t i = j * 32 + lane;
+        v[j] = i < len ? col[b + i] : pad;
+    }
+    warp_bitonic<Id, EL>(v, lane);
+#pragma unroll
+    for (int j = 0; j < EL; ++j) {
+        const uint32_t i = j * 32 + lane;
+        if (i < len) col[b + i] = v[j];
+    }
+}
+
+// Parts of 33..256 entries: one warp each, the register bitonic network.
+template <typename Id>
+__global__ void sort_warp_kernel(uint64_t n, uint32_t d, const int64_t *rowptr,
+                                 const uint32_t *seed_out, Id *col)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    const uint64_t w0 = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    for (uint64_t x0 = w0 * 32; x0 < n; x0 += warps * 32) {
+        const uint64_t x = x0 + lane;
+        uint64_t b = 0, len = 0;
+        if (x < n) in_range<Id>(x, d, rowptr, seed_out, b, len);
+        uint32_t todo = __ballot_sync(kFull, len > 32 && len <= 256);
+        while (todo) {
+            const uint32_t src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const uint64_t sb = __shfl_sync(kFull, b, src);
+            const uint32_t sl = (uint32_t)__shfl_sync(kFull, len, src);
+            if (sl <= 64) warp_sort_part<Id, 2>(col, sb, sl, lane);
+            else if (sl <= 128) warp_sort_part<Id, 4>(col, sb, sl, lane);
+            else warp_sort_part<Id, 8>(col, sb, sl, lane);
+        }
+    }
+}
+
+// Parts of 257..8192 entries: a CTA tests 512 rows at a time, queues those in
+// shared memory and bitonic-sorts each in shared memory.
 template <typename Id>
 __global__ void __launch_bounds__(512) sort_mid_kernel(uint64_t n, uint32_t d, const int64_t *rowptr,
                                                        const uint32_t *seed_out, Id *col)
@@ -284,14 +401,14 @@ __global__ void __launch_bounds__(512) sort_mid_kernel(uint64_t n, uint32_t d, c
         if (x < n) {
             uint64_t b, len;
             in_range<Id>(x, d, rowptr, seed_out, b, len);
-            if (len > 32 && len <= kMidMax) s_rows[atomicAdd(&s_cnt, 1u)] = x;
+            if (len > 256 && len <= kMidMax) s_rows[atomicAdd(&s_cnt, 1u)] = x;
         }
         __syncthreads();
         const uint32_t cnt = s_cnt;
         for (uint32_t m = 0; m < cnt; ++m) {
             uint64_t b, len;
             in_range<Id>(s_rows[m], d, rowptr, seed_out, b, len);
-            uint32_t N = 64;
+            uint32_t N = 512;
             while (N < len) N <<= 1;
             for (uint32_t i = threadIdx.x; i < N; i += blockDim.x)
                 buf[i] = i < len ? col[b + i] : (Id)(~(typename std::make_unsigned<Id>::type)0 >> 1);
@@ -369,12 +486,12 @@ int grid_for(uint64_t items, uint32_t threads, uint32_t per_sm = 8)
 }
 
 struct CsrLayout {
-    uint64_t deg_off, status_off, ctr_off, err_off, seed_out_off, cursor_off, lists_off,
+    uint64_t deg_off, status_off, ctr_off, err_off, seed_out_off, cursor_off, rank_off, lists_off,
         bits_off, counts_off, total;
     uint64_t n_tiles, big_cap, bit_words;
 };
 
-CsrLayout csr_layout(uint64_t n, uint32_t d)
+CsrLayout csr_layout(uint64_t n, uint32_t d, uint64_t n_edges)
 {
     auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
     CsrLayout L{};
@@ -387,7 +504,8 @@ CsrLayout csr_layout(uint64_t n, uint32_t d)
     L.ctr_off = o;        o += 256;                       // scan tile counter + list counters
     L.err_off = o;        o += 256;
     L.seed_out_off = o;   o += al(4 * (d + 1));
-    L.cursor_off = o;     o += al(4 * n);
+    L.cursor_off = o;     o += al(4 * n);                  // in-degree counts
+    L.rank_off = o;       o += al(4 * n_edges);            // rank of each pair in its in part
     L.lists_off = o;      o += al(8 * L.big_cap);
     L.bits_off = o;       o += al(4 * L.bit_words);
     L.counts_off = o;     o += al(8 * (L.bit_words + 1));
@@ -426,29 +544,30 @@ int build_csr(const pa_params *prm, const GenPlan &p, const Id *E, int64_t *rowp
     unsigned long long *ctrs = (unsigned long long *)(scratch + L.ctr_off);
     uint32_t *err = (uint32_t *)(scratch + L.err_off);
 
+    uint32_t *rank = (uint32_t *)(scratch + L.rank_off);
     cudaError_t e = cudaMemsetAsync(err, 0, 4, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(cursor, 0, 4 * n, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(deg + n, 0, 8, s);
     if (e != cudaSuccess) return set_cuda_error(e);
 
-    int rc = pa_degrees(prm, E, deg, s);
-    if (rc != PA_OK) return rc;
-    rc = run_scan(deg, rowptr, n + 1, scratch, L, s);   // deg[n] = 0: rowptr[n] = total
+    seed_out_kernel<Id><<<1, 64, 0, s>>>(E, p.seed_edges, d, seed_out);
+    if (p.n_edges)
+        in_degree_kernel<Id><<<grid_for(p.n_edges, 256), 256, 0, s>>>(E, p.n_edges, n, cursor, rank);
+    deg_fill_kernel<<<grid_for(n + 1, 256), 256, 0, s>>>(cursor, seed_out, n, d, deg);
+    int rc = run_scan(deg, rowptr, n + 1, scratch, L, s);   // deg[n] = 0: rowptr[n] = total
     if (rc != PA_OK) return rc;
 
-    seed_out_kernel<Id><<<1, 64, 0, s>>>(E, p.seed_edges, d, seed_out);
     const uint64_t col_len = 2 * p.n_edges;
     out_part_kernel<Id><<<grid_for(n * d, 256), 256, 0, s>>>(E, rowptr, col, n, d, p.seed_edges,
                                                              col_len);
-    in_part_kernel<Id><<<grid_for(p.n_edges, 256), 256, 0, s>>>(E, p.n_edges, n, d, p.seed_edges,
-                                                                rowptr, cursor, seed_out, col,
-                                                                col_len);
+    in_part_kernel<Id><<<grid_for(p.n_edges, 256), 256, 0, s>>>(E, p.n_edges, n, d, rowptr, rank,
+                                                                seed_out, col, col_len);
     // list counters live after the scan tile counter
     e = cudaMemsetAsync(ctrs + 1, 0, 16, s);
     if (e != cudaSuccess) return set_cuda_error(e);
     unsigned long long *big_list = lists;
     sort_small_kernel<Id><<<grid_for(n, 256), 256, 0, s>>>(n, d, rowptr, seed_out, col, big_list,
                                                            ctrs + 2, L.big_cap);
+    sort_warp_kernel<Id><<<grid_for(n, 256), 256, 0, s>>>(n, d, rowptr, seed_out, col);
     const size_t smem = kMidMax * sizeof(Id);
     e = cudaFuncSetAttribute(sort_mid_kernel<Id>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
@@ -516,7 +635,7 @@ int pa_csr_bytes(const pa_params *prm, uint64_t *rowptr_bytes, uint64_t *col_byt
     if (!rowptr_bytes || !col_bytes || !scratch_bytes) return PA_ERR_INVALID;
     *rowptr_bytes = 8 * (prm->n + 1);
     *col_bytes = 2 * p.n_edges * p.id_bytes;
-    *scratch_bytes = csr_layout(prm->n, prm->d).total;
+    *scratch_bytes = csr_layout(prm->n, prm->d, p.n_edges).total;
     return PA_OK;
 }
 
@@ -527,7 +646,7 @@ int pa_build_csr(const pa_params *prm, const void *d_edges, int64_t *d_rowptr, v
     const int rc = make_plan(prm, &p);
     if (rc != PA_OK) return rc;
     if (!d_edges || !d_rowptr || !d_col || !d_scratch) return PA_ERR_INVALID;
-    const CsrLayout L = csr_layout(prm->n, prm->d);
+    const CsrLayout L = csr_layout(prm->n, prm->d, p.n_edges);
     if (scratch_bytes < L.total) return PA_ERR_CAPACITY;
     if (p.id_bytes == 8)
         return build_csr<int64_t>(prm, p, (const int64_t *)d_edges, d_rowptr, (int64_t *)d_col,

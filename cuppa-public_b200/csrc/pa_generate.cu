@@ -51,326 +51,15 @@
 //    the caller asked for.
 //  * Output: (u, target) pairs.  int64 ids: one 128-bit store per lane; int32
 //    ids: two adjacent lanes' pairs in one 128-bit store.
-#include "pa_device.cuh"
-#include "pa_internal.h"
+#include <vector>
+
+#include "pa_gen_core.cuh"
 
 namespace pa {
 
 namespace {
 
-constexpr uint32_t kFull = 0xffffffffu;
-constexpr uint32_t kThreads = 256;
-constexpr uint32_t kMinBlocks = 4;   // 32 resident warps per SM: at most 64 registers
-
-enum : uint32_t { ST_KNOWN = 0, ST_PEND_GLOBAL = 1, ST_PEND_TILE = 2 };
-
-struct GenArgs {
-    void *edges;
-    GenCtl *ctl;
-    GenRep *reps;
-    uint32_t *flags;
-    uint32_t *sbcnt;      // tiles completed per superblock
-    uint64_t n_sb;
-    uint64_t sb_nodes;    // nodes per superblock
-    uint64_t n;
-    uint64_t u_first;
-    uint64_t n_tiles;
-    uint64_t seed_edges;
-    int64_t slot_off;     // pair index of slot (v, k) = v*d + k + slot_off, for v > d
-    uint64_t pth;
-    uint64_t spin_limit_ns;
-    uint32_t key0, key1;
-    uint32_t d;
-    uint32_t groups;
-    uint32_t tile_nodes;
-    uint32_t seed_mode;
-    uint32_t withhold_first;   // test-only: never publish tile 0
-    uint64_t *trace;           // progress samples (elapsed ns, nodes complete)
-    uint64_t trace_step;       // superblocks between samples
-    uint32_t window_shift;     // start gate: a tile at node tb waits for the watermark
-    uint64_t min_window;       //   to reach tb - max(min_window, tb >> window_shift)
-};
-
-// Record a device-side error once, in the control block and every replica.
-__device__ __forceinline__ void raise_error(const GenArgs &a, uint32_t code)
-{
-    if (atomicCAS(&a.ctl->error, 0u, code) == 0u)
-        for (uint32_t r = 0; r < kReps; ++r) st_relaxed_u32(&a.reps[r].error, code);
-}
-
-// The replica a warp reads.
-__device__ __forceinline__ const GenRep *my_rep(const GenArgs &a)
-{
-    return a.reps + ((blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)) % kReps);
-}
-
-// e-th canonical seed edge.
-__device__ __forceinline__ void seed_edge(uint64_t e, uint32_t d, uint32_t mode, uint64_t &src,
-                                          uint64_t &dst)
-{
-    if (mode == 1) {  // clique: rows v = 1..d hold (v, 0..v-1)
-        uint64_t v = 1, base = 0;
-        while (base + v <= e) { base += v; ++v; }
-        src = v;
-        dst = e - base;
-    } else {          // star node d -> 0..d-1
-        src = d;
-        dst = e;
-    }
-}
-
-// One draw in node arithmetic of width NodeT (see draw_slot in pa_device.cuh;
-// identical values: for u < 2^32, floor(x*u / 2^64) with x = w1:w0 equals
-// floor((w1*u + floor(w0*u / 2^32)) / 2^32)).
-template <typename NodeT>
-struct DrawT {
-    NodeT v;
-    uint32_t k;
-    bool direct;
-};
-
-template <typename NodeT>
-__device__ __forceinline__ DrawT<NodeT> draw(NodeT u, uint32_t i, uint32_t r, const GenArgs &a)
-{
-    DrawT<NodeT> out;
-    if constexpr (sizeof(NodeT) == 4) {
-        const uint4 w = philox4x32_10(make_uint4(u, 0u, i, r), a.key0, a.key1);
-        const uint64_t lo = (uint64_t)w.x * u;
-        const uint64_t hi = (uint64_t)w.y * u + (lo >> 32);
-        out.v = (uint32_t)(hi >> 32);
-        out.k = __umulhi(w.w, a.d);
-        out.direct = (uint64_t)w.z < a.pth;
-    } else {
-        const Draw dr = draw_slot(u, i, r, a.key0, a.key1, a.pth, a.d);
-        out.v = dr.v;
-        out.k = dr.k;
-        out.direct = dr.direct;
-    }
-    return out;
-}
-
-// Per-slot resolution state held in registers.
-template <typename NodeT>
-struct Slot {
-    NodeT val;      // candidate value, or the pending source node v
-    uint32_t meta;  // state (bits 0-1) | k (bits 2-7) | retry (bits 8-31)
-};
-
-__device__ __forceinline__ uint32_t meta_st(uint32_t m) { return m & 3u; }
-__device__ __forceinline__ uint32_t meta_k(uint32_t m) { return (m >> 2) & 63u; }
-__device__ __forceinline__ uint32_t meta_r(uint32_t m) { return m >> 8; }
-
-template <typename Id, typename NodeT>
-__device__ __forceinline__ const Id *slot_addr(const Id *E, const GenArgs &a, NodeT v, uint32_t k)
-{
-    const int64_t idx = (int64_t)((uint64_t)v * a.d) + (int64_t)k + a.slot_off;
-    return E + 2 * idx + 1;
-}
-
-// Where the candidate of a fresh draw comes from.
-template <typename Id, typename NodeT>
-__device__ __forceinline__ void classify(Slot<NodeT> &s, const DrawT<NodeT> &dr, uint32_t r,
-                                         const GenArgs &a, const Id *E, NodeT tb,
-                                         NodeT water_node, uint32_t &n_pend)
-{
-    uint32_t st;
-    if (dr.direct) {
-        s.val = dr.v;
-        st = ST_KNOWN;
-    } else if (dr.v <= a.d) {
-        s.val = (NodeT)seed_slot(dr.v, dr.k, a.d, a.seed_mode);
-        st = ST_KNOWN;
-    } else if (dr.v < water_node) {
-        s.val = (NodeT)ld_slot(slot_addr(E, a, dr.v, dr.k));
-        st = ST_KNOWN;
-    } else if (dr.v < tb) {
-        s.val = dr.v;
-        st = ST_PEND_GLOBAL;
-        ++n_pend;
-    } else {
-        s.val = dr.v;
-        st = ST_PEND_TILE;
-    }
-    s.meta = st | (dr.k << 2) | (r << 8);
-}
-
-// Per-warp constants of one launch.
-struct Lane {
-    uint32_t lane, g, slot, gmask, lt, le;
-    bool used;
-};
-
-// Stage 1: retry-0 draws of every slot of tile t, early copy loads.
-template <typename Id, typename NodeT, int P>
-__device__ __forceinline__ void stage1(Slot<NodeT> (&s)[P], uint64_t t, const GenArgs &a,
-                                       const Id *E, const Lane &L, NodeT water_node,
-                                       uint32_t &n_pend)
-{
-    const NodeT tb = (NodeT)(a.u_first + t * a.tile_nodes);
-    const NodeT te = (NodeT)min(a.n, (uint64_t)tb + a.tile_nodes);
-#pragma unroll
-    for (int j = 0; j < P; ++j) {
-        const NodeT u = tb + (NodeT)(j * a.groups + L.g);
-        s[j].val = 0;
-        s[j].meta = ST_KNOWN;
-        if (L.used && u < te)
-            classify(s[j], draw<NodeT>(u, L.slot, 0u, a), 0u, a, E, tb, water_node, n_pend);
-    }
-}
-
-// Resolve the slots of one warp pass until every active lane is final.
-// Returns false when the warp must stop (wait limit, or another warp failed).
-template <typename Id, typename NodeT>
-__device__ __forceinline__ bool resolve_pass(Slot<NodeT> &s, const GenArgs &a, const Id *E,
-                                             const Id *tilebuf, NodeT tb, NodeT pbase,
-                                             uint32_t pass_off, NodeT u, bool active,
-                                             const Lane &L, NodeT &water_node,
-                                             uint32_t &n_retry, uint32_t &n_wait,
-                                             uint32_t &n_pend, uint32_t &n_poll)
-{
-    const uint32_t d = a.d;
-    uint64_t spin_t0 = 0;
-    uint32_t sleep_ns = 64;
-    for (;;) {
-        bool changed = false;
-        const uint32_t st0 = meta_st(s.meta);
-        const uint32_t k = meta_k(s.meta);
-        if (active && st0 == ST_PEND_GLOBAL) {
-            const NodeT v = s.val;
-            bool ready = v < water_node;
-            if (!ready)
-                ready = ld_acquire_u32(a.flags + ((uint64_t)v - a.u_first) / a.tile_nodes) != 0u;
-            if (!ready) ++n_poll;
-            if (ready) {
-                s.val = (NodeT)ld_slot(slot_addr(E, a, v, k));
-                s.meta &= ~3u;
-                changed = true;
-            }
-        } else if (active && st0 == ST_PEND_TILE) {
-            const NodeT off = s.val - tb;
-            if (off < (NodeT)pass_off) {   // a finished earlier pass of this tile
-                s.val = (NodeT)tilebuf[(uint32_t)off * d + k];
-                s.meta &= ~3u;
-                changed = true;
-            }
-        }
-
-        const bool known = active && meta_st(s.meta) == ST_KNOWN;
-        uint32_t eq;
-        if constexpr (sizeof(NodeT) == 4) {
-            // values < 2^32 - 32: the lane-unique keys of unknown lanes never collide
-            eq = __match_any_sync(kFull, known ? (uint32_t)s.val : (0xffffffe0u | L.lane));
-        } else {
-            eq = __match_any_sync(kFull, known ? (unsigned long long)s.val
-                                               : (0x8000000000000000ull | L.lane));
-        }
-        const bool bad = active && (!known || (eq & L.lt & L.gmask) != 0u);
-        const uint32_t badm = __ballot_sync(kFull, bad);
-        const bool fin = active && (badm & L.gmask & L.le) == 0u;
-        const uint32_t finm = __ballot_sync(kFull, fin || !active);
-        if (finm == kFull) return true;
-
-        // Copy targets in this same pass: take the source lane's value once
-        // that lane is final.
-        const bool same = active && meta_st(s.meta) == ST_PEND_TILE && s.val >= pbase;
-        const uint32_t src = same ? (uint32_t)(s.val - pbase) * d + k : L.lane;
-        const NodeT sv = __shfl_sync(kFull, s.val, src);
-        if (same && ((finm >> src) & 1u)) {
-            s.val = sv;
-            s.meta &= ~3u;
-            changed = true;
-        }
-
-        // A candidate equal to a final lower slot is rejected for certain.
-        if (known && !fin && (eq & L.lt & L.gmask & finm) != 0u) {
-            const uint32_t r = meta_r(s.meta) + 1u;
-            classify(s, draw<NodeT>(u, L.slot, r, a), r, a, E, tb, water_node, n_pend);
-            changed = true;
-            ++n_retry;
-        }
-
-        if (!__any_sync(kFull, changed)) {
-            // Nothing moved: every open slot waits on another tile.
-            unsigned long long now = 0, w2 = 0;
-            uint32_t err = 0;
-            if (L.lane == 0) {
-                now = globaltimer_ns();
-                const GenRep *rp = my_rep(a);
-                err = ld_relaxed_u32(&rp->error);
-                w2 = ld_acquire_u64(&rp->water);
-                ++n_wait;
-            }
-            now = __shfl_sync(kFull, now, 0);
-            err = __shfl_sync(kFull, err, 0);
-            w2 = __shfl_sync(kFull, w2, 0);
-            __syncwarp();
-            water_node = (NodeT)(a.u_first + w2 * a.sb_nodes);
-            if (spin_t0 == 0) spin_t0 = now;
-            if (err != 0) return false;
-            if (now - spin_t0 > a.spin_limit_ns) {
-                if (L.lane == 0) raise_error(a, (uint32_t)PA_ERR_SPIN_TIMEOUT);
-                return false;
-            }
-            __nanosleep(sleep_ns);
-            sleep_ns = min(sleep_ns * 2u, 1024u);
-        } else {
-            spin_t0 = 0;
-            sleep_ns = 64;
-        }
-    }
-}
-
-// Stage 2: resolve, store and publish tile t.
-template <typename Id, typename NodeT, int P>
-__device__ __forceinline__ bool stage2(Slot<NodeT> (&s)[P], uint64_t t, const GenArgs &a, Id *E,
-                                       Id *tilebuf, const Lane &L, NodeT &water_node,
-                                       uint32_t &n_retry, uint32_t &n_wait, uint32_t &n_pend,
-                                       uint32_t &n_poll)
-{
-    const uint32_t d = a.d, G = a.groups;
-    const NodeT tb = (NodeT)(a.u_first + t * a.tile_nodes);
-    const NodeT te = (NodeT)min(a.n, (uint64_t)tb + a.tile_nodes);
-#pragma unroll
-    for (int j = 0; j < P; ++j) {
-        const NodeT pbase = tb + (NodeT)(j * G);   // first node of the pass
-        const NodeT u = pbase + (NodeT)L.g;
-        const bool active = L.used && u < te;
-        if (!resolve_pass(s[j], a, E, tilebuf, tb, pbase, (uint32_t)j * G, u, active, L,
-                          water_node, n_retry, n_wait, n_pend, n_poll))
-            return false;
-        // Finished pass: keep it for in-tile copy reads, then emit the edges.
-        if (active) tilebuf[(uint32_t)j * G * d + L.lane] = (Id)s[j].val;
-        __syncwarp();
-        const uint64_t e0 = a.seed_edges + ((uint64_t)pbase - a.u_first) * d;
-        if constexpr (sizeof(Id) == 8) {
-            if (active) st_pair(E + 2 * (e0 + L.lane), (uint64_t)u, (uint64_t)s[j].val);
-        } else {
-            const uint32_t nu = __shfl_down_sync(kFull, (uint32_t)u, 1);
-            const uint32_t nv = __shfl_down_sync(kFull, (uint32_t)s[j].val, 1);
-            const uint32_t na = __shfl_down_sync(kFull, (uint32_t)active, 1);
-            const bool leader = ((L.lane + (uint32_t)(e0 & 1u)) & 1u) == 0u;
-            if (active) {
-                Id *p = E + 2 * (e0 + L.lane);
-                if (leader) {
-                    if (L.lane < 31u && na) st_pair2(p, u, s[j].val, nu, nv);
-                    else st_pair(p, u, s[j].val);
-                } else if (L.lane == 0) {
-                    st_pair(p, u, s[j].val);
-                }
-            }
-        }
-    }
-
-    // Publish.  The warp barrier orders every lane's stores before lane 0's
-    // release fence; the flag and the superblock count are written after it.
-    __syncwarp();
-    if (L.lane == 0 && !(a.withhold_first && t == 0)) {
-        fence_acq_rel_gpu();
-        st_relaxed_u32(a.flags + t, 1u);
-        red_add_relaxed_u32(a.sbcnt + t / kSbTiles, 1u);
-    }
-    return true;
-}
+using namespace gen;
 
 // The single writer of the completion watermark.  Each round trip reads the
 // tile counts of 128 consecutive superblocks (one 16-byte load per lane),
@@ -380,7 +69,10 @@ __device__ __forceinline__ bool stage2(Slot<NodeT> (&s)[P], uint64_t t, const Ge
 // the same limit, so a stall that long means they have stopped).
 __device__ __forceinline__ void advance_watermark(const GenArgs &a, uint32_t lane)
 {
-    uint64_t w = 0;
+    // Tiles before tile_begin were generated by the level launches that ran
+    // before this launch: publish that prefix first.
+    uint64_t w = a.water_init;
+    if (lane <= kReps) st_relaxed_u64(lane < kReps ? &a.reps[lane].water : &a.ctl->water, w);
     uint64_t t0 = globaltimer_ns();
     const uint64_t t_start = t0;
     uint64_t next_sample = 0;
@@ -451,7 +143,7 @@ __device__ __forceinline__ uint64_t claim_next(Claimer &c, const GenArgs &a, con
     if (c.idx == kClaimTiles) {
         const uint64_t chunk = __shfl_sync(kFull, c.pre, 0);
         if (L.lane == 0) c.pre = atomicAdd(&a.ctl->ticket, 1ull);
-        c.base = chunk * kClaimTiles;
+        c.base = a.tile_begin + chunk * kClaimTiles;
         c.idx = 0;
     }
     return c.base + c.idx++;
@@ -662,6 +354,78 @@ int launch_passes(const GenArgs &a, uint32_t passes, uint32_t blocks, cudaStream
     return PA_ERR_INVALID;
 }
 
+// Level tables of one graph, written on the device from kernel parameters so
+// that pa_generate needs no host-to-device copy (and no host synchronization).
+struct LevelInit {
+    GenArgs a;
+    uint32_t levels;
+    unsigned long long bounds[kMaxLevels + 1];
+};
+
+struct LevelArea {
+    uint64_t args_off, lvl_off, ibase_off, lstart_off, ticket_off;
+};
+
+constexpr LevelArea level_area()
+{
+    return LevelArea{0, 256, 256 + 8 * (kMaxLevels + 1), 256 + 8 * (kMaxLevels + 1) + 16 * kMaxLevels,
+                     256 + 8 * (kMaxLevels + 1) + 16 * kMaxLevels + 4 * kMaxLevels + 16};
+}
+static_assert(level_area().ticket_off + 8 * (kMaxLevels + 1) <= kLevelAreaBytes, "level area");
+
+__global__ void init_levels_kernel(const LevelInit li, unsigned char *area)
+{
+    constexpr LevelArea A = level_area();
+    if (threadIdx.x == 0) *reinterpret_cast<GenArgs *>(area + A.args_off) = li.a;
+    unsigned long long *lvl = reinterpret_cast<unsigned long long *>(area + A.lvl_off);
+    unsigned long long *ib = reinterpret_cast<unsigned long long *>(area + A.ibase_off);
+    unsigned int *ls = reinterpret_cast<unsigned int *>(area + A.lstart_off);
+    for (uint32_t l = threadIdx.x; l <= li.levels; l += blockDim.x) {
+        lvl[l] = li.bounds[l];
+        if (l < li.levels) {
+            ib[2 * l] = 0;
+            ib[2 * l + 1] = li.bounds[l + 1] - li.bounds[l];
+            ls[l] = (unsigned int)li.bounds[l];
+        }
+    }
+}
+
+// Levels [0, split) of one graph, one launch each (the batch kernel with one
+// instance); returns the first tile left to the persistent launch.
+int run_early_levels(const GenArgs &a, const GenPlan &plan, unsigned char *scratch,
+                     cudaStream_t stream, uint64_t &tile_begin)
+{
+    tile_begin = 0;
+    const std::vector<uint64_t> bd = level_bounds(plan.u_first, a.n, plan.n_tiles, plan.tile_nodes);
+    const uint32_t levels = (uint32_t)bd.size() - 1;
+    uint32_t split = split_levels(bd, plan.u_first, plan.tile_nodes);
+    if (split == 0 || levels > kMaxLevels) return PA_OK;
+    LevelInit li;
+    li.a = a;
+    li.a.max_sleep_ns = 1024;
+    li.levels = levels;
+    for (uint32_t l = 0; l <= levels; ++l) li.bounds[l] = bd[l];
+    unsigned char *area = scratch + plan.level_offset;
+    init_levels_kernel<<<1, 128, 0, stream>>>(li, area);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_cuda_error(e);
+    constexpr LevelArea A = level_area();
+    LevelTables tabs;
+    tabs.lvl_base = reinterpret_cast<const unsigned long long *>(area + A.lvl_off);
+    tabs.inst_base = reinterpret_cast<const unsigned long long *>(area + A.ibase_off);
+    tabs.loc_start = reinterpret_cast<const unsigned int *>(area + A.lstart_off);
+    tabs.levels = levels;
+    const GenArgs *d_inst = reinterpret_cast<const GenArgs *>(area + A.args_off);
+    unsigned long long *tickets = reinterpret_cast<unsigned long long *>(area + A.ticket_off);
+    for (uint32_t l = 0; l < split; ++l) {
+        const int rc = launch_levels(plan.id_bytes, plan.passes, d_inst, tabs, 1, l, bd[l], bd[l + 1],
+                                     tickets + l, a.ctl, stream);
+        if (rc != PA_OK) return rc;
+    }
+    tile_begin = bd[split];
+    return PA_OK;
+}
+
 }  // namespace
 
 int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, void *d_scratch,
@@ -695,13 +459,28 @@ int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, vo
     a.trace = reinterpret_cast<uint64_t *>(reinterpret_cast<unsigned char *>(d_scratch) + plan.trace_offset);
     a.trace_step = (plan.n_sb + kTraceMax - 1) / kTraceMax;
     if (a.trace_step == 0) a.trace_step = 1;
+    a.max_sleep_ns = 1024;
     a.window_shift = 3;
     a.min_window = 16384;
+    a.tile_begin = 0;
+    a.water_init = 0;
 
     const uint32_t blocks = blocks_override ? blocks_override : prm->blocks;
     // 32-bit node arithmetic needs every node id, and tile base + tile_nodes,
     // below 2^32 - 32 (the top 32 values are the unknown-lane match keys).
     const bool small = prm->n + plan.tile_nodes + 32 < (1ull << 32);
+    // The start of the graph, level by level (32-bit node arithmetic only, and
+    // not with a caller-chosen grid, which the tests use to exercise the
+    // persistent launch on its own).
+    if (small && plan.passes <= 4 && blocks == 0) {
+        uint64_t tb = 0;
+        const int rc = run_early_levels(a, plan, reinterpret_cast<unsigned char *>(d_scratch), stream, tb);
+        if (rc != PA_OK) return rc;
+        a.tile_begin = tb;
+        a.water_init = tb / kSbTiles;
+        // (with no early level the persistent launch still writes the seed edges)
+        if (tb > 0 && tb >= plan.n_tiles) return PA_OK;
+    }
     if (plan.id_bytes == 8)
         return small ? launch_passes<int64_t, uint32_t>(a, plan.passes, blocks, stream)
                      : launch_passes<int64_t, uint64_t>(a, plan.passes, blocks, stream);

@@ -41,6 +41,7 @@ constexpr uint64_t kCtlBytes = kRepOffset + kReps * 128;    // flags start here
 constexpr uint32_t kSbTiles = 64;    // tiles per superblock (watermark granularity)
 constexpr uint32_t kClaimTiles = 4;  // consecutive tiles claimed by one ticket
 constexpr uint32_t kTraceMax = 2048; // progress samples kept per generation
+constexpr uint64_t kLevelAreaBytes = 8192;  // level-launch tables of one graph
 
 // Resolved launch geometry of one generation.
 struct GenPlan {
@@ -53,6 +54,7 @@ struct GenPlan {
     uint64_t n_sb;          // superblocks of kSbTiles tiles
     uint64_t sb_offset;     // byte offset of the superblock counters in the scratch
     uint64_t trace_offset;  // byte offset of the progress trace in the scratch
+    uint64_t level_offset;  // byte offset of the level-launch tables in the scratch
     uint64_t seed_edges;
     uint64_t n_edges;
     uint64_t pth;           // direct threshold

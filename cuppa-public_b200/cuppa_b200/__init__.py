@@ -131,6 +131,11 @@ _SIGS = {
                                       ctypes.c_int, ctypes.c_void_p]),
     "pa_write_degree_distribution": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p,
                                                     ctypes.c_char_p, ctypes.c_void_p]),
+    "pa_batch_scratch_bytes": (ctypes.c_int, [_P(PaParams), ctypes.c_uint32,
+                                              _P(ctypes.c_uint64)]),
+    "pa_batch_generate": (ctypes.c_int, [_P(PaParams), ctypes.c_uint32, _P(ctypes.c_void_p),
+                                         _P(ctypes.c_uint64), ctypes.c_void_p, ctypes.c_uint64,
+                                         ctypes.c_void_p]),
     "pa_graph_create": (ctypes.c_int, [_P(PaParams), _P(PaGraph)]),
     "pa_graph_generate": (ctypes.c_int, [_P(PaGraph), ctypes.c_void_p, _P(PaStats)]),
     "pa_graph_destroy": (ctypes.c_int, [_P(PaGraph)]),
@@ -250,6 +255,38 @@ def generate(prm: PaParams, stream=None, raise_on_error: bool = True):
     if raise_on_error:
         check(st.status, "pa_generate (device)")
     return edges[: edge_count(prm)], st
+
+
+class Batch:
+    """Device buffers for a batch of graphs generated by one persistent launch."""
+
+    def __init__(self, prms, device=None):
+        torch = _torch()
+        self.prms = list(prms)
+        k = len(self.prms)
+        self._arr = (PaParams * k)(*self.prms)
+        sb = ctypes.c_uint64()
+        check(lib().pa_batch_scratch_bytes(self._arr, k, ctypes.byref(sb)), "pa_batch_scratch_bytes")
+        self.scratch = torch.empty(sb.value, dtype=torch.uint8, device=device or "cuda")
+        self.edges = []
+        for prm in self.prms:
+            dt = torch.int64 if prm.id_bits == 64 else torch.int32
+            self.edges.append(torch.empty((max(edge_count(prm), 1), 2), dtype=dt,
+                                          device=device or "cuda"))
+        self._ptrs = (ctypes.c_void_p * k)(*[e.data_ptr() for e in self.edges])
+        self._bytes = (ctypes.c_uint64 * k)(*[e.numel() * e.element_size() for e in self.edges])
+
+    def generate(self, stream=None) -> None:
+        check(lib().pa_batch_generate(self._arr, len(self.prms), self._ptrs, self._bytes,
+                                      ctypes.c_void_p(self.scratch.data_ptr()),
+                                      self.scratch.numel(), ctypes.c_void_p(_stream_ptr(stream))),
+              "pa_batch_generate")
+
+    def finish(self, stream=None) -> PaStats:
+        return finish(self.scratch, stream)
+
+    def graph(self, i: int):
+        return self.edges[i][: edge_count(self.prms[i])]
 
 
 def canonicalize(prm: PaParams, edges, out=None, stream=None):

@@ -154,6 +154,20 @@ int pa_csr_bytes(const pa_params *prm, uint64_t *rowptr_bytes, uint64_t *col_byt
 int pa_build_csr(const pa_params *prm, const void *d_edges, int64_t *d_rowptr, void *d_col,
                  void *d_scratch, uint64_t scratch_bytes, void *stream);
 
+/* ---- batches ---------------------------------------------------------------- */
+/* Many independent graphs in one persistent launch (no counterpart in the
+ * reference, which makes one graph per run).  prms[i] describes graph i (all of
+ * one id width, every n < 2^32 - 64; tile_passes is taken from prms[0]); graph i
+ * is written to d_edges[i] (edges_bytes[i] >= pa_edges_bytes(prms[i])) exactly as
+ * pa_generate would write it.  The graphs' tiles are claimed in the order given:
+ * list large graphs first.  The call copies a small table to the device and
+ * waits for that copy, then returns with the launch queued; read the status with
+ * pa_generate_finish(d_scratch, ...). */
+int pa_batch_scratch_bytes(const pa_params *prms, uint32_t count, uint64_t *bytes);
+int pa_batch_generate(const pa_params *prms, uint32_t count, void *const *d_edges,
+                      const uint64_t *edges_bytes, void *d_scratch, uint64_t scratch_bytes,
+                      void *stream);
+
 /* ---- files ------------------------------------------------------------------ */
 enum { PA_FORMAT_TEXT = 0, PA_FORMAT_BINARY = 1 };
 /* Write the device edge list to `path`: TEXT = one "u v" line per pair, the

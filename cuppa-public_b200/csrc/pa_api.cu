@@ -30,6 +30,15 @@ static uint64_t p_threshold(double p)
     return t > (1ull << 32) ? (1ull << 32) : t;
 }
 
+uint64_t start_split(uint64_t n, uint64_t u_first, uint64_t sb_nodes, uint64_t want)
+{
+    // The start kernel runs 32-bit node arithmetic: keep it well below 2^32.
+    if (want > (1ull << 31)) want = 1ull << 31;
+    const uint64_t avail = n > u_first ? n - u_first : 0;
+    const uint64_t span = (want + sb_nodes - 1) / sb_nodes * sb_nodes;
+    return u_first + (span < avail ? span : avail);
+}
+
 int make_plan(const pa_params *prm, GenPlan *plan)
 {
     const int rc = pa_params_check(prm);
@@ -49,9 +58,13 @@ int make_plan(const pa_params *prm, GenPlan *plan)
     p.n_sb = (p.n_tiles + kSbTiles - 1) / kSbTiles;
     p.sb_offset = kCtlBytes + ((p.n_tiles * 4ull + 255ull) & ~255ull);
     p.trace_offset = p.sb_offset + ((p.n_sb * 4ull + 255ull) & ~255ull);
-    p.level_offset = p.trace_offset + (uint64_t)kTraceMax * 16ull;
-    p.scratch_bytes = p.level_offset + kLevelAreaBytes;
+    p.start_offset = p.trace_offset + (uint64_t)kTraceMax * 16ull;
+    p.scratch_bytes = p.start_offset + kStartAreaBytes;
     p.spin_limit_ns = prm->spin_limit_ns ? prm->spin_limit_ns : 2000000000ull;
+    const uint64_t want = prm->start_nodes == PA_START_NONE ? 0
+                          : prm->start_nodes ? prm->start_nodes
+                                             : kStartNodesAuto;
+    p.u_split = start_split(prm->n, p.u_first, (uint64_t)kSbTiles * p.tile_nodes, want);
     *plan = p;
     return PA_OK;
 }

@@ -1,27 +1,21 @@
-// pa_batch.cu -- many independent graphs, and the start of every graph, by
-// level launches.
+// pa_batch.cu -- many independent graphs in shared launches.
 //
-// The north star's batching: instances of uneven size (n, d, p, seed, seed
-// graph) share launches instead of one launch each, so the long dependency
-// chains at the start of every graph run side by side and the launch and tail
-// costs are paid once.  No reference counterpart (the reference generates one
-// graph per process run, src/main.cu:105-116).
+// Instances of uneven size (n, d, p, seed, seed graph) share launches instead of
+// one launch each, so the dependency chains at the start of every graph run
+// side by side and the launch and tail costs are paid once.  No reference
+// counterpart (the reference generates one graph per process run,
+// src/main.cu:105-116).
 //
-//  * Levels (pa_gen_core.cuh): level l of a graph covers nodes
-//    [B_l, B_{l+1}), B_{l+1} = B_l + max(4096, B_l / 8).  The tiles of all
-//    instances form one index space ordered by level and, within a level, by
-//    instance.  A warp claims four tiles at a time from the launch's ticket and
-//    maps a tile to (level, instance, tile of the instance) by two binary
-//    searches over prefix tables.
-//  * Every level that starts below 2^21 nodes is its own launch.  The launch
-//    boundary is a barrier: when level l starts, everything below it is
-//    complete, so copy reads below B_l need no check at all and only the reads
-//    into level l itself (about 1/9 of them) wait on tile flags.  The remaining
-//    levels run as one launch, in which a copy read above the launch's start
-//    checks the completion count of its source's superblock (64 tiles; the
-//    counts of a whole batch are L2-resident) before it reads.
-//  * Each instance's tiles are claimed in increasing order by running warps, so
-//    every instance is deadlock-free exactly as in the single-graph kernel.
+//  * One fill launch sets the start region of every instance to all-ones.
+//  * One start-kernel launch (pa_start.cu) generates every instance's start
+//    region, with slot-granular waits, the warp passes of all instances in
+//    level order (pa_gen_core.cuh).
+//  * One tail launch of the batch kernel below generates the rest of the
+//    instances that are larger than their start region, tiles in level order.
+//    Everything below an instance's start_end is complete when it starts, so
+//    only copy reads at or above it check the completion count of the source's
+//    superblock (64 tiles; the counts of a whole batch are L2-resident) and, if
+//    that is not complete, poll the source tile's flag.
 //  * A warp keeps its current instance's arguments in shared memory; the slot
 //    code is the single-graph kernel's (pa_gen_core.cuh).
 #include <algorithm>
@@ -33,26 +27,18 @@
 namespace pa {
 namespace gen {
 
-std::vector<uint64_t> level_bounds(uint64_t u_first, uint64_t n, uint64_t n_tiles,
-                                   uint64_t tile_nodes)
+std::vector<uint64_t> level_bounds(uint64_t u_first, uint64_t lo, uint64_t n_end,
+                                   uint64_t unit_nodes)
 {
-    std::vector<uint64_t> out{0};
-    uint64_t B = u_first;
-    while (out.back() < n_tiles) {
+    auto units = [&](uint64_t node) { return (node - u_first + unit_nodes - 1) / unit_nodes; };
+    const uint64_t n_units = units(n_end);
+    std::vector<uint64_t> out{units(lo)};
+    uint64_t B = lo;
+    while (out.back() < n_units) {
         B += std::max<uint64_t>(kLevelMinNodes, B >> kLevelShift);
-        const uint64_t nb = B >= n ? n : B;
-        uint64_t t = (nb - u_first + tile_nodes - 1) / tile_nodes;
-        if (t > n_tiles) t = n_tiles;
-        out.push_back(t);
+        out.push_back(std::min(units(std::min(B, n_end)), n_units));
     }
     return out;
-}
-
-uint32_t split_levels(const std::vector<uint64_t> &bounds, uint64_t u_first, uint64_t tile_nodes)
-{
-    uint32_t l = 0;
-    while (l + 1 < bounds.size() && u_first + bounds[l] * tile_nodes < kSplitNodes) ++l;
-    return l;
 }
 
 }  // namespace gen
@@ -65,35 +51,10 @@ struct BatchArgs {
     const GenArgs *inst;                    // per-instance arguments (device)
     LevelTables tab;
     uint32_t count;
-    uint32_t l_begin;                       // first level of this launch
     unsigned long long t_begin, t_end;      // global tiles of this launch
     unsigned long long *ticket;             // this launch's claim counter
     GenCtl *ctl;                            // shared status and counters
 };
-
-// Largest index i in [0, len) with a[i] <= x (a ascending, a[0] <= x).
-__device__ __forceinline__ uint32_t last_le(const unsigned long long *a, uint32_t len,
-                                            unsigned long long x)
-{
-    uint32_t lo = 0, hi = len;
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (__ldg(a + mid) <= x) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
-
-// Global tile T -> (instance, tile of the instance).
-__device__ __forceinline__ void map_tile(const BatchArgs &b, unsigned long long T, uint32_t &inst,
-                                         uint64_t &t)
-{
-    const uint32_t l = last_le(b.tab.lvl_base, b.tab.levels, T);
-    const unsigned long long r = T - __ldg(b.tab.lvl_base + l);
-    const unsigned long long *ib = b.tab.inst_base + (uint64_t)l * (b.count + 1);
-    inst = last_le(ib, b.count, r);
-    t = __ldg(b.tab.loc_start + (uint64_t)l * b.count + inst) + (r - __ldg(ib + inst));
-}
 
 template <typename Id, int P>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) batch_kernel(const BatchArgs b)
@@ -111,24 +72,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) batch_kernel(const Batch
     uint32_t cur = 0xffffffffu;
     uint32_t water_node = 0;
 
-    // The launch that starts at level 0 writes every instance's seed edges
-    // (closed forms; nothing reads them back).
-    if (b.l_begin == 0) {
-        const uint32_t gw = blockIdx.x * (kThreads / 32) + warp;
-        const uint32_t nw = gridDim.x * (kThreads / 32);
-        for (uint32_t i = gw; i < b.count; i += nw) {
-            const GenArgs *ai = b.inst + i;
-            Id *Ei = reinterpret_cast<Id *>(ai->edges);
-            const uint32_t di = ai->d, mode = ai->seed_mode;
-            const uint64_t se = ai->seed_edges;
-            for (uint64_t e = L.lane; e < se; e += 32) {
-                uint64_t s, u;
-                seed_edge(e, di, mode, s, u);
-                st_pair(Ei + 2 * e, s, u);
-            }
-        }
-    }
-
     uint32_t n_retry = 0, n_wait = 0, n_done = 0, n_pend = 0, n_poll = 0;
     bool ok = true;
     while (ok) {
@@ -142,7 +85,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) batch_kernel(const Batch
             if (T >= b.t_end) break;
             uint32_t i;
             uint64_t t;
-            map_tile(b, T, i, t);
+            map_unit(b.tab, b.count, T, i, t);
             if (i != cur) {
                 // copy the instance's arguments into this warp's shared slot
                 __syncwarp();
@@ -155,11 +98,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) batch_kernel(const Batch
                 L.slot = L.lane - L.g * a.d;
                 L.used = L.lane < a.groups * a.d;
                 L.gmask = L.used ? (a.d == 32 ? kFull : (((1u << a.d) - 1u) << (L.g * a.d))) : 0u;
-                // everything below this launch's first level is complete
-                water_node = (uint32_t)(a.u_first +
-                                        (uint64_t)__ldg(b.tab.loc_start +
-                                                        (uint64_t)b.l_begin * b.count + i) *
-                                            a.tile_nodes);
+                // everything below the instance's start region end is complete
+                water_node = (uint32_t)a.start_end;
             }
             Id *E = reinterpret_cast<Id *>(a.edges);
             Slot<uint32_t> S[P];
@@ -211,21 +151,19 @@ int launch_batch(const BatchArgs &b, cudaStream_t s)
 
 namespace gen {
 
-int launch_levels(uint32_t id_bytes, uint32_t passes, const GenArgs *d_inst, const LevelTables &tabs,
-                  uint32_t count, uint32_t l_begin, unsigned long long t_begin,
-                  unsigned long long t_end, unsigned long long *d_ticket, GenCtl *ctl,
-                  cudaStream_t s)
+int launch_tail(uint32_t id_bytes, uint32_t passes, const GenArgs *d_inst, const LevelTables &tabs,
+                uint32_t count, unsigned long long t_begin, unsigned long long t_end,
+                unsigned long long *d_ticket, GenCtl *ctl, cudaStream_t s)
 {
     BatchArgs b;
     b.inst = d_inst;
     b.tab = tabs;
     b.count = count;
-    b.l_begin = l_begin;
     b.t_begin = t_begin;
     b.t_end = t_end;
     b.ticket = d_ticket;
     b.ctl = ctl;
-    if (t_end <= t_begin && l_begin != 0) return PA_OK;
+    if (t_end <= t_begin) return PA_OK;
     if (id_bytes == 8) {
         switch (passes) {
         case 1: return launch_batch<int64_t, 1>(b, s);
@@ -246,17 +184,49 @@ int launch_levels(uint32_t id_bytes, uint32_t passes, const GenArgs *d_inst, con
 
 namespace {
 
-// Scratch layout of a batch.
-struct BatchLayout {
-    uint64_t table_off, lvl_off, ibase_off, lstart_off, ticket_off, inst_off, total;
-    uint32_t levels, split;
-    std::vector<uint64_t> flags_off, sb_off;
-    std::vector<GenPlan> plans;
-    std::vector<std::vector<uint64_t>> bounds;   // per instance: tile index at each level start
+// Level tables of one launch over a set of instances (host side).
+struct HostLevels {
+    uint32_t levels = 0;
+    std::vector<unsigned long long> lvl, ibase, lstart;
+    uint64_t lvl_off = 0, ibase_off = 0, lstart_off = 0;   // device copies in the scratch
 };
 
-// One pass per tile by default: small tiles keep the dependency chains at the
-// start of each graph short.
+// bounds[i]: unit bounds of instance i's levels (level_bounds).  Global order:
+// level by level, instance by instance.
+void build_levels(const std::vector<std::vector<uint64_t>> &bounds, HostLevels &H)
+{
+    const uint32_t count = (uint32_t)bounds.size();
+    H.levels = 1;
+    for (const auto &bd : bounds) H.levels = std::max<uint32_t>(H.levels, (uint32_t)bd.size() - 1);
+    const uint32_t Lv = H.levels;
+    H.lvl.assign(Lv + 1, 0);
+    H.ibase.assign((uint64_t)Lv * (count + 1), 0);
+    H.lstart.assign((uint64_t)Lv * count, 0);
+    for (uint32_t l = 0; l < Lv; ++l) {
+        unsigned long long acc = 0;
+        for (uint32_t i = 0; i < count; ++i) {
+            const auto &bd = bounds[i];
+            const uint64_t lo = l < bd.size() ? bd[l] : bd.back();
+            const uint64_t hi = l + 1 < bd.size() ? bd[l + 1] : bd.back();
+            H.ibase[(uint64_t)l * (count + 1) + i] = acc;
+            H.lstart[(uint64_t)l * count + i] = lo;
+            acc += hi - lo;
+        }
+        H.ibase[(uint64_t)l * (count + 1) + count] = acc;
+        H.lvl[l + 1] = H.lvl[l] + acc;
+    }
+}
+
+// Scratch layout of a batch.
+struct BatchLayout {
+    uint64_t table_off, ticket_off, inst_off, total;
+    std::vector<uint64_t> flags_off, sb_off;
+    std::vector<GenPlan> plans;
+    HostLevels start, tail;
+    uint64_t max_start_pairs;
+};
+
+// One pass per tile by default: small tiles keep the dependency chains short.
 uint32_t batch_passes(const pa_params *prms) { return prms[0].tile_passes ? prms[0].tile_passes : 1u; }
 
 int batch_layout(const pa_params *prms, uint32_t count, BatchLayout &L)
@@ -267,38 +237,37 @@ int batch_layout(const pa_params *prms, uint32_t count, BatchLayout &L)
     L.plans.resize(count);
     L.flags_off.resize(count);
     L.sb_off.resize(count);
-    L.bounds.resize(count);
-    uint64_t o = kCtlBytes;
-    L.table_off = o;
-    o += al((uint64_t)count * sizeof(GenArgs));
+    L.max_start_pairs = 0;
+    std::vector<std::vector<uint64_t>> sb(count), tb(count);
     for (uint32_t i = 0; i < count; ++i) {
         pa_params q = prms[i];
         q.tile_passes = P;   // one pass count per launch
         const int rc = make_plan(&q, &L.plans[i]);
         if (rc != PA_OK) return rc;
+        const GenPlan &p = L.plans[i];
         if (prms[i].id_bits != prms[0].id_bits) return PA_ERR_INVALID;
-        if (prms[i].n + L.plans[i].tile_nodes + 32 >= (1ull << 32)) return PA_ERR_NOT_SUPPORTED;
+        if (prms[i].n + p.tile_nodes + 32 >= (1ull << 32)) return PA_ERR_NOT_SUPPORTED;
         if (prms[i].flags != 0) return PA_ERR_INVALID;
-        if (L.plans[i].n_tiles >= (1ull << 32)) return PA_ERR_NOT_SUPPORTED;
-        L.bounds[i] = level_bounds(L.plans[i].u_first, prms[i].n, L.plans[i].n_tiles,
-                                   L.plans[i].tile_nodes);
+        sb[i] = level_bounds(p.u_first, p.u_first, p.u_split, (uint64_t)kStartPasses * p.groups);
+        tb[i] = level_bounds(p.u_first, p.u_split, prms[i].n, p.tile_nodes);
+        L.max_start_pairs = std::max<uint64_t>(L.max_start_pairs, (p.u_split - p.u_first) * prms[i].d);
     }
-    L.levels = 1;
-    L.split = 0;
-    for (uint32_t i = 0; i < count; ++i) {
-        L.levels = std::max<uint32_t>(L.levels, (uint32_t)L.bounds[i].size() - 1);
-        L.split = std::max<uint32_t>(
-            L.split, split_levels(L.bounds[i], L.plans[i].u_first, L.plans[i].tile_nodes));
+    build_levels(sb, L.start);
+    build_levels(tb, L.tail);
+    if (L.start.levels > kMaxLevels || L.tail.levels > kMaxLevels) return PA_ERR_NOT_SUPPORTED;
+    uint64_t o = kCtlBytes;
+    L.table_off = o;
+    o += al((uint64_t)count * sizeof(GenArgs));
+    for (HostLevels *H : {&L.start, &L.tail}) {
+        H->lvl_off = o;
+        o += al(8ull * H->lvl.size());
+        H->ibase_off = o;
+        o += al(8ull * H->ibase.size());
+        H->lstart_off = o;
+        o += al(8ull * H->lstart.size());
     }
-    if (L.levels > kMaxLevels) return PA_ERR_NOT_SUPPORTED;
-    L.lvl_off = o;
-    o += al(8ull * (L.levels + 1));
-    L.ibase_off = o;
-    o += al(8ull * L.levels * (count + 1));
-    L.lstart_off = o;
-    o += al(4ull * L.levels * count);
     L.ticket_off = o;
-    o += al(8ull * (kMaxLevels + 1));
+    o += 256;
     L.inst_off = o;
     for (uint32_t i = 0; i < count; ++i) {
         L.flags_off[i] = o;
@@ -308,6 +277,16 @@ int batch_layout(const pa_params *prms, uint32_t count, BatchLayout &L)
     }
     L.total = o;
     return PA_OK;
+}
+
+gen::LevelTables device_tables(const HostLevels &H, unsigned char *scr)
+{
+    gen::LevelTables t;
+    t.lvl_base = reinterpret_cast<const unsigned long long *>(scr + H.lvl_off);
+    t.inst_base = reinterpret_cast<const unsigned long long *>(scr + H.ibase_off);
+    t.loc_start = reinterpret_cast<const unsigned long long *>(scr + H.lstart_off);
+    t.levels = H.levels;
+    return t;
 }
 
 }  // namespace
@@ -336,6 +315,7 @@ int pa_batch_generate(const pa_params *prms, uint32_t count, void *const *d_edge
     if (rc != PA_OK) return rc;
     if (!d_edges || !edges_bytes || !d_scratch) return PA_ERR_INVALID;
     if (scratch_bytes < L.total) return PA_ERR_CAPACITY;
+    if (reinterpret_cast<uintptr_t>(d_scratch) & 15u) return PA_ERR_INVALID;
     const uint32_t P = batch_passes(prms);
     if (P != 1 && P != 2 && P != 4) return PA_ERR_NOT_SUPPORTED;
     unsigned char *scr = (unsigned char *)d_scratch;
@@ -369,23 +349,7 @@ int pa_batch_generate(const pa_params *prms, uint32_t count, void *const *d_edge
         a.max_sleep_ns = 4096;   // many warps wait at once: keep their polls sparse
         a.window_shift = 63;
         a.min_window = 0;
-    }
-    // level tables: global order is level by level, instance by instance
-    const uint32_t Lv = L.levels;
-    std::vector<unsigned long long> lvl(Lv + 1, 0), ibase((uint64_t)Lv * (count + 1), 0);
-    std::vector<unsigned int> lstart((uint64_t)Lv * count, 0);
-    for (uint32_t l = 0; l < Lv; ++l) {
-        unsigned long long acc = 0;
-        for (uint32_t i = 0; i < count; ++i) {
-            const auto &bd = L.bounds[i];
-            const uint64_t lo = l < bd.size() ? bd[l] : bd.back();
-            const uint64_t hi = l + 1 < bd.size() ? bd[l + 1] : bd.back();
-            ibase[(uint64_t)l * (count + 1) + i] = acc;
-            lstart[(uint64_t)l * count + i] = (unsigned int)lo;
-            acc += hi - lo;
-        }
-        ibase[(uint64_t)l * (count + 1) + count] = acc;
-        lvl[l + 1] = lvl[l] + acc;
+        a.start_end = p.u_split;
     }
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = cudaMemsetAsync(scr, 0, kCtlBytes, s);
@@ -393,38 +357,41 @@ int pa_batch_generate(const pa_params *prms, uint32_t count, void *const *d_edge
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(scr + L.table_off, table.data(), count * sizeof(gen::GenArgs),
                             cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(scr + L.lvl_off, lvl.data(), lvl.size() * 8ull, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(scr + L.ibase_off, ibase.data(), ibase.size() * 8ull,
-                            cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(scr + L.lstart_off, lstart.data(), lstart.size() * 4ull,
-                            cudaMemcpyHostToDevice, s);
+    for (const HostLevels *H : {&L.start, &L.tail}) {
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(scr + H->lvl_off, H->lvl.data(), H->lvl.size() * 8ull,
+                                cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(scr + H->ibase_off, H->ibase.data(), H->ibase.size() * 8ull,
+                                cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(scr + H->lstart_off, H->lstart.data(), H->lstart.size() * 8ull,
+                                cudaMemcpyHostToDevice, s);
+    }
     // the host vectors are pageable: make sure the copies have read them
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return set_cuda_error(e);
 
-    gen::LevelTables tabs;
-    tabs.lvl_base = reinterpret_cast<const unsigned long long *>(scr + L.lvl_off);
-    tabs.inst_base = reinterpret_cast<const unsigned long long *>(scr + L.ibase_off);
-    tabs.loc_start = reinterpret_cast<const unsigned int *>(scr + L.lstart_off);
-    tabs.levels = Lv;
     const gen::GenArgs *d_inst = reinterpret_cast<const gen::GenArgs *>(scr + L.table_off);
     unsigned long long *tickets = reinterpret_cast<unsigned long long *>(scr + L.ticket_off);
     GenCtl *ctl = reinterpret_cast<GenCtl *>(scr);
     const uint32_t id_bytes = prms[0].id_bits / 8;
-    // one launch per early level, then the rest in one launch
-    const uint32_t split = std::min(L.split, Lv);
-    for (uint32_t l = 0; l < split; ++l) {
-        rc = gen::launch_levels(id_bytes, P, d_inst, tabs, count, l, lvl[l], lvl[l + 1], tickets + l,
-                                ctl, s);
-        if (rc != PA_OK) return rc;
-    }
-    if (split < Lv || split == 0)
-        rc = gen::launch_levels(id_bytes, P, d_inst, tabs, count, split, lvl[split], lvl[Lv],
-                                tickets + split, ctl, s);
-    return rc;
+    rc = gen::fill_start(id_bytes, d_inst, count, L.max_start_pairs, s);
+    if (rc != PA_OK) return rc;
+    gen::StartArgs sa;
+    std::memset(&sa, 0, sizeof(sa));
+    sa.inst = d_inst;
+    sa.tab = device_tables(L.start, scr);
+    sa.count = count;
+    sa.write_seeds = 1;
+    sa.t_end = L.start.lvl[L.start.levels];
+    sa.ticket = tickets;
+    sa.ctl = ctl;
+    if (count == 1) sa.one = table[0];
+    rc = gen::launch_start(id_bytes, sa, 0, s);
+    if (rc != PA_OK) return rc;
+    return gen::launch_tail(id_bytes, P, d_inst, device_tables(L.tail, scr), count,
+                            L.tail.lvl[0], L.tail.lvl[L.tail.levels], tickets + 1, ctl, s);
 }
 
 }  // extern "C"

@@ -186,6 +186,21 @@ __device__ __forceinline__ void st_pair(int32_t *p, uint64_t a, uint64_t b)
                  : "memory");
 }
 
+// gpu-scope relaxed pair stores: the start kernel's readers poll the second
+// field of a pair while its writer may still be running.
+__device__ __forceinline__ void st_relaxed_pair(int64_t *p, uint64_t a, uint64_t b)
+{
+    asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(a), "l"(b)
+                 : "memory");
+}
+
+__device__ __forceinline__ void st_relaxed_pair(int32_t *p, uint64_t a, uint64_t b)
+{
+    asm volatile("st.relaxed.gpu.global.v2.u32 [%0], {%1, %2};" ::"l"(p), "r"((uint32_t)a),
+                 "r"((uint32_t)b)
+                 : "memory");
+}
+
 __device__ __forceinline__ void st_pair2(int32_t *p, uint64_t a, uint64_t b, uint64_t c, uint64_t d)
 {
     asm volatile("st.global.v4.u32 [%0], {%1, %2, %3, %4};" ::"l"(p), "r"((uint32_t)a),

@@ -46,6 +46,7 @@ struct GenArgs {
     uint64_t water_init;       // superblocks complete when the persistent launch starts
     uint32_t window_shift;     // start gate: a tile at node tb waits for the watermark
     uint64_t min_window;       //   to reach tb - max(min_window, tb >> window_shift)
+    uint64_t start_end;        // start kernel: nodes [u_first, start_end) are its work
 };
 
 // Record a device-side error once, in the control block and every replica.
@@ -362,46 +363,91 @@ __device__ __forceinline__ bool stage2(Slot<NodeT> (&s)[P], uint64_t t, const Ge
 }  // namespace pa
 
 // ---------------------------------------------------------------------------
-// Level launches (pa_batch.cu).  The first part of every graph is generated
-// level by level, one launch per level: level l covers nodes
-// [B_l, B_{l+1}), B_{l+1} = B_l + max(kLevelMinNodes, B_l >> kLevelShift), so a
-// level's copy reads fall below the level (already complete: the previous
-// launch has finished) except for a share of about 1/9, which waits on tile
-// flags inside the launch.  Levels that start at or above kSplitNodes are left
-// to one launch (the batch kernel for batches, the pipelined persistent kernel
-// for a single graph).
+// Level-ordered index spaces of several graphs, and the two extra launches.
+//
+// Level l of a graph covers nodes [B_l, B_{l+1}), B_{l+1} = B_l +
+// max(kLevelMinNodes, B_l >> kLevelShift).  The units (tiles or passes) of
+// several graphs form one index space ordered by level and, within a level, by
+// graph, so the start of every graph is worked on first and side by side.
+// Within one graph the order is increasing, which is what deadlock freedom
+// needs (a unit waits only on lower units of its own graph).
 // ---------------------------------------------------------------------------
 namespace pa {
 namespace gen {
 
 constexpr uint64_t kLevelMinNodes = 4096;
 constexpr uint32_t kLevelShift = 3;
-constexpr uint64_t kSplitNodes = 1ull << 21;
 constexpr uint32_t kMaxLevels = 160;
 
-// Device copies of the level tables of a set of instances.
+// Device copies of the level tables of a set of graphs.
 struct LevelTables {
-    const unsigned long long *lvl_base;    // levels + 1: first global tile of each level
+    const unsigned long long *lvl_base;    // levels + 1: first global unit of each level
     const unsigned long long *inst_base;   // levels x (count + 1): prefix within a level
-    const unsigned int *loc_start;         // levels x count: instance's first tile of a level
+    const unsigned long long *loc_start;   // levels x count: graph's first unit of a level
     uint32_t levels;
 };
 
-// Tile bounds of a graph's levels: entry l is the first tile of level l, the
-// last entry is n_tiles.
-std::vector<uint64_t> level_bounds(uint64_t u_first, uint64_t n, uint64_t n_tiles,
-                                   uint64_t tile_nodes);
+// Unit bounds of a graph's levels over nodes [u_first, n_end) in units of
+// unit_nodes: entry l is the first unit of level l, the last is n_units.
+std::vector<uint64_t> level_bounds(uint64_t u_first, uint64_t n_end, uint64_t n_units,
+                                   uint64_t unit_nodes);
 
-// Number of levels that start below kSplitNodes (each gets its own launch).
-uint32_t split_levels(const std::vector<uint64_t> &bounds, uint64_t u_first, uint64_t tile_nodes);
+// Largest index i in [0, len) with a[i] <= x (a ascending, a[0] <= x).
+__device__ __forceinline__ uint32_t last_le(const unsigned long long *a, uint32_t len,
+                                            unsigned long long x)
+{
+    uint32_t lo = 0, hi = len;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(a + mid) <= x) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
 
-// One launch of the batch kernel over global tiles [t_begin, t_end), which
-// belong to levels >= l_begin (all tiles of every instance below its level
-// l_begin start are complete when the launch starts).
-int launch_levels(uint32_t id_bytes, uint32_t passes, const GenArgs *d_inst, const LevelTables &tabs,
-                  uint32_t count, uint32_t l_begin, unsigned long long t_begin,
-                  unsigned long long t_end, unsigned long long *d_ticket, GenCtl *ctl,
-                  cudaStream_t s);
+// Global unit T -> (graph, unit of the graph).
+__device__ __forceinline__ void map_unit(const LevelTables &tab, uint32_t count,
+                                         unsigned long long T, uint32_t &inst, uint64_t &t)
+{
+    const uint32_t l = last_le(tab.lvl_base, tab.levels, T);
+    const unsigned long long r = T - __ldg(tab.lvl_base + l);
+    const unsigned long long *ib = tab.inst_base + (uint64_t)l * (count + 1);
+    inst = last_le(ib, count, r);
+    t = __ldg(tab.loc_start + (uint64_t)l * count + inst) + (r - __ldg(ib + inst));
+}
+
+// Warp passes per start tile, the start kernel's unit of work.
+constexpr int kStartPasses = 4;
+
+// Start kernel (pa_start.cu): start tiles of one graph (count == 1, arguments in
+// `one`) or of `count` graphs in level order (arguments in `inst`).
+struct StartArgs {
+    GenArgs one;
+    const GenArgs *inst;
+    LevelTables tab;
+    uint32_t count;
+    uint32_t write_seeds;          // also write every graph's seed edges
+    unsigned long long t_end;      // start tiles of the launch
+    unsigned long long *ticket;    // claim counter (zero at launch)
+    GenCtl *ctl;                   // shared status and counters
+};
+
+// Launch the start kernel; `blocks` 0 = one wave.  The target field of every
+// pair of the graphs' start regions must hold all-ones before it runs.
+int launch_start(uint32_t id_bytes, const StartArgs &b, uint32_t blocks, cudaStream_t s);
+
+// Set every byte of the pairs of nodes [u_first, start_end) of each of `count`
+// graphs to 0xff (one launch).
+int fill_start(uint32_t id_bytes, const GenArgs *d_inst, uint32_t count, uint64_t max_pairs,
+               cudaStream_t s);
+
+// Batch kernel (pa_batch.cu) over global tiles [t_begin, t_end) of `count`
+// graphs; every node of graph i below node u_first + loc_start[l_begin][i] *
+// tile_nodes is complete when it starts.
+int launch_tail(uint32_t id_bytes, uint32_t passes, const GenArgs *d_inst, const LevelTables &tabs,
+                uint32_t count, uint32_t l_begin, unsigned long long t_begin,
+                unsigned long long t_end, unsigned long long *d_ticket, GenCtl *ctl,
+                cudaStream_t s);
 
 }  // namespace gen
 }  // namespace pa

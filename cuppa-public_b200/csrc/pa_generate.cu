@@ -51,7 +51,7 @@
 //    the caller asked for.
 //  * Output: (u, target) pairs.  int64 ids: one 128-bit store per lane; int32
 //    ids: two adjacent lanes' pairs in one 128-bit store.
-#include <vector>
+#include <cstring>
 
 #include "pa_gen_core.cuh"
 
@@ -69,7 +69,7 @@ using namespace gen;
 // the same limit, so a stall that long means they have stopped).
 __device__ __forceinline__ void advance_watermark(const GenArgs &a, uint32_t lane)
 {
-    // Tiles before tile_begin were generated by the level launches that ran
+    // Tiles before tile_begin were generated by the start kernel, which ran
     // before this launch: publish that prefix first.
     uint64_t w = a.water_init;
     if (lane <= kReps) st_relaxed_u64(lane < kReps ? &a.reps[lane].water : &a.ctl->water, w);
@@ -287,6 +287,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) gen_kernel(const GenArgs
     uint64_t t_next = claim_next(cl, a, L);
     wt = __shfl_sync(kFull, wt, 0);
     __syncwarp();   // orders lane 0's acquire before every lane's slot loads
+    if (wt < a.water_init) wt = a.water_init;   // the start kernel's nodes
     NodeT water_node = (NodeT)(a.u_first + wt * a.sb_nodes);
 
     Slot<NodeT> A[P], B[P];
@@ -354,78 +355,6 @@ int launch_passes(const GenArgs &a, uint32_t passes, uint32_t blocks, cudaStream
     return PA_ERR_INVALID;
 }
 
-// Level tables of one graph, written on the device from kernel parameters so
-// that pa_generate needs no host-to-device copy (and no host synchronization).
-struct LevelInit {
-    GenArgs a;
-    uint32_t levels;
-    unsigned long long bounds[kMaxLevels + 1];
-};
-
-struct LevelArea {
-    uint64_t args_off, lvl_off, ibase_off, lstart_off, ticket_off;
-};
-
-constexpr LevelArea level_area()
-{
-    return LevelArea{0, 256, 256 + 8 * (kMaxLevels + 1), 256 + 8 * (kMaxLevels + 1) + 16 * kMaxLevels,
-                     256 + 8 * (kMaxLevels + 1) + 16 * kMaxLevels + 4 * kMaxLevels + 16};
-}
-static_assert(level_area().ticket_off + 8 * (kMaxLevels + 1) <= kLevelAreaBytes, "level area");
-
-__global__ void init_levels_kernel(const LevelInit li, unsigned char *area)
-{
-    constexpr LevelArea A = level_area();
-    if (threadIdx.x == 0) *reinterpret_cast<GenArgs *>(area + A.args_off) = li.a;
-    unsigned long long *lvl = reinterpret_cast<unsigned long long *>(area + A.lvl_off);
-    unsigned long long *ib = reinterpret_cast<unsigned long long *>(area + A.ibase_off);
-    unsigned int *ls = reinterpret_cast<unsigned int *>(area + A.lstart_off);
-    for (uint32_t l = threadIdx.x; l <= li.levels; l += blockDim.x) {
-        lvl[l] = li.bounds[l];
-        if (l < li.levels) {
-            ib[2 * l] = 0;
-            ib[2 * l + 1] = li.bounds[l + 1] - li.bounds[l];
-            ls[l] = (unsigned int)li.bounds[l];
-        }
-    }
-}
-
-// Levels [0, split) of one graph, one launch each (the batch kernel with one
-// instance); returns the first tile left to the persistent launch.
-int run_early_levels(const GenArgs &a, const GenPlan &plan, unsigned char *scratch,
-                     cudaStream_t stream, uint64_t &tile_begin)
-{
-    tile_begin = 0;
-    const std::vector<uint64_t> bd = level_bounds(plan.u_first, a.n, plan.n_tiles, plan.tile_nodes);
-    const uint32_t levels = (uint32_t)bd.size() - 1;
-    uint32_t split = split_levels(bd, plan.u_first, plan.tile_nodes);
-    if (split == 0 || levels > kMaxLevels) return PA_OK;
-    LevelInit li;
-    li.a = a;
-    li.a.max_sleep_ns = 1024;
-    li.levels = levels;
-    for (uint32_t l = 0; l <= levels; ++l) li.bounds[l] = bd[l];
-    unsigned char *area = scratch + plan.level_offset;
-    init_levels_kernel<<<1, 128, 0, stream>>>(li, area);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return set_cuda_error(e);
-    constexpr LevelArea A = level_area();
-    LevelTables tabs;
-    tabs.lvl_base = reinterpret_cast<const unsigned long long *>(area + A.lvl_off);
-    tabs.inst_base = reinterpret_cast<const unsigned long long *>(area + A.ibase_off);
-    tabs.loc_start = reinterpret_cast<const unsigned int *>(area + A.lstart_off);
-    tabs.levels = levels;
-    const GenArgs *d_inst = reinterpret_cast<const GenArgs *>(area + A.args_off);
-    unsigned long long *tickets = reinterpret_cast<unsigned long long *>(area + A.ticket_off);
-    for (uint32_t l = 0; l < split; ++l) {
-        const int rc = launch_levels(plan.id_bytes, plan.passes, d_inst, tabs, 1, l, bd[l], bd[l + 1],
-                                     tickets + l, a.ctl, stream);
-        if (rc != PA_OK) return rc;
-    }
-    tile_begin = bd[split];
-    return PA_OK;
-}
-
 }  // namespace
 
 int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, void *d_scratch,
@@ -465,21 +394,35 @@ int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, vo
     a.tile_begin = 0;
     a.water_init = 0;
 
+    a.start_end = plan.u_split;
+
     const uint32_t blocks = blocks_override ? blocks_override : prm->blocks;
     // 32-bit node arithmetic needs every node id, and tile base + tile_nodes,
     // below 2^32 - 32 (the top 32 values are the unknown-lane match keys).
     const bool small = prm->n + plan.tile_nodes + 32 < (1ull << 32);
-    // The start of the graph, level by level (32-bit node arithmetic only, and
-    // not with a caller-chosen grid, which the tests use to exercise the
-    // persistent launch on its own).
-    if (small && plan.passes <= 4 && blocks == 0) {
-        uint64_t tb = 0;
-        const int rc = run_early_levels(a, plan, reinterpret_cast<unsigned char *>(d_scratch), stream, tb);
+    if (plan.u_split > plan.u_first) {
+        // The start region, with slot-granular waits (pa_start.cu): its pairs
+        // start as all-ones, the start kernel writes them and the seed edges.
+        const uint64_t pair_bytes = 2ull * plan.id_bytes;
+        e = cudaMemsetAsync(reinterpret_cast<unsigned char *>(d_edges) + plan.seed_edges * pair_bytes,
+                            0xff, (plan.u_split - plan.u_first) * prm->d * pair_bytes, stream);
+        if (e != cudaSuccess) return set_cuda_error(e);
+        StartArgs sa;
+        std::memset(&sa, 0, sizeof(sa));
+        sa.one = a;
+        sa.count = 1;
+        sa.write_seeds = 1;
+        const uint64_t st_nodes = (uint64_t)kStartPasses * plan.groups;
+        sa.t_end = (plan.u_split - plan.u_first + st_nodes - 1) / st_nodes;
+        sa.ticket = reinterpret_cast<unsigned long long *>(reinterpret_cast<unsigned char *>(d_scratch) +
+                                                          plan.start_offset);
+        sa.ctl = a.ctl;
+        const int rc = launch_start(plan.id_bytes, sa, blocks, stream);
         if (rc != PA_OK) return rc;
-        a.tile_begin = tb;
-        a.water_init = tb / kSbTiles;
-        // (with no early level the persistent launch still writes the seed edges)
-        if (tb > 0 && tb >= plan.n_tiles) return PA_OK;
+        if (plan.u_split >= prm->n) return PA_OK;
+        // u_split - u_first is a whole number of superblocks
+        a.tile_begin = (plan.u_split - plan.u_first) / plan.tile_nodes;
+        a.water_init = a.tile_begin / kSbTiles;
     }
     if (plan.id_bytes == 8)
         return small ? launch_passes<int64_t, uint32_t>(a, plan.passes, blocks, stream)

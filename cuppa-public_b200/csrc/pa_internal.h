@@ -41,7 +41,7 @@ constexpr uint64_t kCtlBytes = kRepOffset + kReps * 128;    // flags start here
 constexpr uint32_t kSbTiles = 64;    // tiles per superblock (watermark granularity)
 constexpr uint32_t kClaimTiles = 4;  // consecutive tiles claimed by one ticket
 constexpr uint32_t kTraceMax = 2048; // progress samples kept per generation
-constexpr uint64_t kLevelAreaBytes = 8192;  // level-launch tables of one graph
+constexpr uint64_t kStartAreaBytes = 256;  // the start kernel's claim counter
 
 // Resolved launch geometry of one generation.
 struct GenPlan {
@@ -54,7 +54,8 @@ struct GenPlan {
     uint64_t n_sb;          // superblocks of kSbTiles tiles
     uint64_t sb_offset;     // byte offset of the superblock counters in the scratch
     uint64_t trace_offset;  // byte offset of the progress trace in the scratch
-    uint64_t level_offset;  // byte offset of the level-launch tables in the scratch
+    uint64_t start_offset;  // byte offset of the start kernel's claim counter
+    uint64_t u_split;       // nodes [u_first, u_split) are the start kernel's
     uint64_t seed_edges;
     uint64_t n_edges;
     uint64_t pth;           // direct threshold
@@ -67,6 +68,13 @@ struct GenPlan {
 int set_cuda_error(cudaError_t e);
 
 int make_plan(const pa_params *prm, GenPlan *plan);
+
+// Start region of a graph: nodes [u_first, u_split) with u_split - u_first the
+// smallest whole number of superblocks covering `want` nodes, capped at n.
+uint64_t start_split(uint64_t n, uint64_t u_first, uint64_t sb_nodes, uint64_t want);
+
+// Default start region: the first 2^24 generated nodes.
+constexpr uint64_t kStartNodesAuto = 1ull << 24;
 
 // Launch the generator kernel on `stream` into caller memory; scratch must hold
 // plan.scratch_bytes and is cleared here.

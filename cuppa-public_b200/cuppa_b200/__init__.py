@@ -49,6 +49,8 @@ PA_FORMAT_BINARY = 1
 # Test-only: the generator never publishes its first tile, so every wait on it
 # runs into the wait limit (a flag that nothing sets).
 PA_FLAG_TEST_WITHHOLD_FIRST_TILE = 1 << 31
+# start_nodes: no start kernel (every node in the persistent launch)
+PA_START_NONE = (1 << 64) - 1
 
 
 class CuppaError(RuntimeError):
@@ -71,6 +73,7 @@ class PaParams(ctypes.Structure):
         ("tile_passes", ctypes.c_uint32),
         ("flags", ctypes.c_uint32),
         ("spin_limit_ns", ctypes.c_uint64),
+        ("start_nodes", ctypes.c_uint64),
     ]
 
 
@@ -172,13 +175,14 @@ def check(status: int, where: str) -> None:
 
 def make_params(n: int, d: int, p: float, seed: int = 42, id_bits: int = 32,
                 seed_mode: int = PA_SEED_CLIQUE, blocks: int = 0, threads: int = 0,
-                tile_passes: int = 0, flags: int = 0, spin_limit_ns: int = 0) -> PaParams:
+                tile_passes: int = 0, flags: int = 0, spin_limit_ns: int = 0,
+                start_nodes: int = 0) -> PaParams:
     prm = PaParams()
     check(lib().pa_params_init(ctypes.byref(prm)), "pa_params_init")
     prm.n, prm.d, prm.p, prm.seed = n, d, float(p), seed
     prm.id_bits, prm.seed_mode = id_bits, seed_mode
     prm.blocks, prm.threads, prm.tile_passes = blocks, threads, tile_passes
-    prm.flags, prm.spin_limit_ns = flags, spin_limit_ns
+    prm.flags, prm.spin_limit_ns, prm.start_nodes = flags, spin_limit_ns, start_nodes
     return prm
 
 

@@ -59,6 +59,8 @@ enum { PA_LAYOUT_PAIRS = 0 };
  * the generator never publishes its first tile, so every wait on that tile runs
  * into spin_limit_ns and the call reports PA_ERR_SPIN_TIMEOUT. */
 #define PA_FLAG_TEST_WITHHOLD_FIRST_TILE 0x80000000u
+/* (with a start kernel, its first warp pass is withheld instead: the first
+ *  nodes' slots are never written, with the same outcome) */
 
 typedef struct pa_params {
     uint64_t n;             /* nodes                        (-n/--n1; cuPPA(n, ...))      */
@@ -73,7 +75,13 @@ typedef struct pa_params {
     uint32_t tile_passes;   /* warp passes per claimed tile (1, 2, 4 or 8); 0 = auto      */
     uint32_t flags;         /* PA_FLAG_* (0 for normal use)                               */
     uint64_t spin_limit_ns; /* limit of any single device wait; 0 = 2 s                    */
+    uint64_t start_nodes;   /* nodes after the seed generated by the start kernel (slot-
+                               granular waits); rounded up to whole superblocks of the
+                               persistent launch.  0 = auto, PA_START_NONE = none        */
 } pa_params;
+
+/* pa_params.start_nodes: no start kernel (the persistent launch does every node). */
+#define PA_START_NONE UINT64_MAX
 
 /* Statistics and device-side status of one generation. */
 typedef struct pa_stats {

@@ -10,7 +10,10 @@ import _oracle as orc
 pytestmark = pytest.mark.gpu
 
 
-def _mixed(pa, count, rng, max_n=200_000, bits=32):
+def _mixed(pa, count, rng, max_n=200_000, bits=32, mixed_start=False):
+    """Random instances; with mixed_start each instance's start region is, at
+    random, the default (the whole graph), none, or 1500 nodes (so the tail
+    launch runs too)."""
     prms = []
     for i in range(count):
         n = int(round(10 ** rng.uniform(1.2, np.log10(max_n))))
@@ -18,15 +21,18 @@ def _mixed(pa, count, rng, max_n=200_000, bits=32):
         n = max(n, d + 1)
         p = float(rng.uniform(0.1, 0.9))
         mode = int(rng.integers(0, 2))
-        prms.append(pa.make_params(n, d, p, seed=1000 + i, id_bits=bits, seed_mode=mode))
+        sn = [0, pa.PA_START_NONE, 1500][int(rng.integers(0, 3))] if mixed_start else 0
+        prms.append(pa.make_params(n, d, p, seed=1000 + i, id_bits=bits, seed_mode=mode,
+                                   start_nodes=sn))
     prms.sort(key=lambda q: -q.n * q.d)   # large graphs first
     return prms
 
 
+@pytest.mark.parametrize("mixed_start", [False, True])
 @pytest.mark.parametrize("bits", [32, 64])
-def test_batch_equals_single_graph_runs(pa, cuda_ok, bits):
+def test_batch_equals_single_graph_runs(pa, cuda_ok, bits, mixed_start):
     rng = np.random.default_rng(5)
-    prms = _mixed(pa, 60, rng, bits=bits)
+    prms = _mixed(pa, 60, rng, bits=bits, mixed_start=mixed_start)
     batch = pa.Batch(prms)
     batch.generate()
     st = batch.finish()

@@ -46,25 +46,42 @@ for d in (4, 16):
             SWEEP.append((50000, d, 0.5, 2 ** 33 + d, mode, bits))
 
 
+# How the nodes are split between the start kernel (slot-granular waits) and the
+# persistent kernel (tile flags and the watermark): the default (every node of
+# these small graphs in the start kernel), none in it, and a boundary inside the
+# graph (2000 nodes, rounded up to whole superblocks).
+START = {"start": 0, "persistent": None, "split": 2000}
+
+
+def start_nodes(pa, which):
+    v = START[which]
+    return pa.PA_START_NONE if v is None else v
+
+
+@pytest.mark.parametrize("start", list(START))
 @pytest.mark.parametrize("n,d,p,seed,mode,bits", SWEEP)
-def test_bit_exact_sweep(pa, cuda_ok, n, d, p, seed, mode, bits):
+def test_bit_exact_sweep(pa, cuda_ok, n, d, p, seed, mode, bits, start):
     if n < d + 1:
         pytest.skip("fewer than d+1 nodes")
-    assert_bit_exact(pa, n, d, p, seed, mode, bits)
+    assert_bit_exact(pa, n, d, p, seed, mode, bits, start_nodes=start_nodes(pa, start))
 
 
+@pytest.mark.parametrize("start", ["persistent", "split"])
 @pytest.mark.parametrize("passes", [1, 2, 4, 8])
 @pytest.mark.parametrize("d", [3, 4, 16])
-def test_bit_exact_every_tile_shape(pa, cuda_ok, passes, d):
-    assert_bit_exact(pa, 30000, d, 0.4, 9, 1, 32, tile_passes=passes)
-    assert_bit_exact(pa, 30000, d, 0.0, 9, 0, 64, tile_passes=passes)
+def test_bit_exact_every_tile_shape(pa, cuda_ok, passes, d, start):
+    sn = start_nodes(pa, start)
+    assert_bit_exact(pa, 30000, d, 0.4, 9, 1, 32, tile_passes=passes, start_nodes=sn)
+    assert_bit_exact(pa, 30000, d, 0.0, 9, 0, 64, tile_passes=passes, start_nodes=sn)
 
 
+@pytest.mark.parametrize("start", list(START))
 @pytest.mark.parametrize("blocks", [1, 2, 3, 7, 4000])
-def test_any_grid_size_is_deadlock_free_and_exact(pa, cuda_ok, blocks):
-    """Tiles are claimed in order by running warps, so a single CTA, or far more
+def test_any_grid_size_is_deadlock_free_and_exact(pa, cuda_ok, blocks, start):
+    """Work is claimed in order by running warps, so a single CTA, or far more
     CTAs than fit at once, still finish with the same bits."""
-    assert_bit_exact(pa, 20000, 4, 0.3, 5, 1, 32, blocks=blocks)
+    assert_bit_exact(pa, 20000, 4, 0.3, 5, 1, 32, blocks=blocks,
+                     start_nodes=start_nodes(pa, start))
 
 
 def test_benchmark_cpu_config_matches_golden(pa, cuda_ok):
@@ -104,9 +121,10 @@ def test_canonicalize_and_degrees(pa, cuda_ok, bits, d):
     assert (edges.cpu().numpy() == orc.pairs_canonical(G, mode)).all()
 
 
-def test_million_node_bit_exact(pa, cuda_ok):
-    assert_bit_exact(pa, 1_000_000, 4, 0.5, 1234, 1, 64)
-    assert_bit_exact(pa, 1_000_000, 4, 0.0, 1234, 1, 64)
+@pytest.mark.parametrize("start", [0, 100_000])
+def test_million_node_bit_exact(pa, cuda_ok, start):
+    assert_bit_exact(pa, 1_000_000, 4, 0.5, 1234, 1, 64, start_nodes=start)
+    assert_bit_exact(pa, 1_000_000, 4, 0.0, 1234, 1, 64, start_nodes=start)
 
 
 def test_repeatable_and_stream_ordered(pa, cuda_ok):
@@ -121,12 +139,13 @@ def test_repeatable_and_stream_ordered(pa, cuda_ok):
     assert s1.retries == s2.retries
 
 
-def test_wait_limit_reports_error_and_context_survives(pa, cuda_ok):
-    """The first tile is never published (a flag nothing sets): every wait on it
-    ends at the 20 ms limit, the call returns PA_ERR_SPIN_TIMEOUT, and the
-    context stays usable for the next generation."""
+@pytest.mark.parametrize("start", list(START))
+def test_wait_limit_reports_error_and_context_survives(pa, cuda_ok, start):
+    """The first tile (or, in the start kernel, the first warp pass) is never
+    published: every wait on it ends at the 20 ms limit, the call returns
+    PA_ERR_SPIN_TIMEOUT, and the context stays usable for the next generation."""
     prm = pa.make_params(200000, 4, 0.2, seed=1, flags=pa.PA_FLAG_TEST_WITHHOLD_FIRST_TILE,
-                         spin_limit_ns=20_000_000)
+                         spin_limit_ns=20_000_000, start_nodes=start_nodes(pa, start))
     edges, st = pa.generate(prm, raise_on_error=False)
     assert st.status == pa.PA_ERR_SPIN_TIMEOUT
     with pytest.raises(pa.CuppaError):

@@ -22,7 +22,7 @@
 #include <cstring>
 #include <vector>
 
-#include "pa_gen_core.cuh"
+#include "pa_batch.h"
 
 namespace pa {
 namespace gen {
@@ -184,16 +184,9 @@ int launch_tail(uint32_t id_bytes, uint32_t passes, const GenArgs *d_inst, const
 
 namespace {
 
-// Level tables of one launch over a set of instances (host side).
-struct HostLevels {
-    uint32_t levels = 0;
-    std::vector<unsigned long long> lvl, ibase, lstart;
-    uint64_t lvl_off = 0, ibase_off = 0, lstart_off = 0;   // device copies in the scratch
-};
-
 // bounds[i]: unit bounds of instance i's levels (level_bounds).  Global order:
 // level by level, instance by instance.
-void build_levels(const std::vector<std::vector<uint64_t>> &bounds, HostLevels &H)
+void build_levels(const std::vector<std::vector<uint64_t>> &bounds, BatchLevels &H)
 {
     const uint32_t count = (uint32_t)bounds.size();
     H.levels = 1;
@@ -217,69 +210,7 @@ void build_levels(const std::vector<std::vector<uint64_t>> &bounds, HostLevels &
     }
 }
 
-// Scratch layout of a batch.
-struct BatchLayout {
-    uint64_t table_off, ticket_off, inst_off, total;
-    std::vector<uint64_t> flags_off, sb_off;
-    std::vector<GenPlan> plans;
-    HostLevels start, tail;
-    uint64_t max_start_pairs;
-};
-
-// One pass per tile by default: small tiles keep the dependency chains short.
-uint32_t batch_passes(const pa_params *prms) { return prms[0].tile_passes ? prms[0].tile_passes : 1u; }
-
-int batch_layout(const pa_params *prms, uint32_t count, BatchLayout &L)
-{
-    if (!prms || count == 0) return PA_ERR_INVALID;
-    auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
-    const uint32_t P = batch_passes(prms);
-    L.plans.resize(count);
-    L.flags_off.resize(count);
-    L.sb_off.resize(count);
-    L.max_start_pairs = 0;
-    std::vector<std::vector<uint64_t>> sb(count), tb(count);
-    for (uint32_t i = 0; i < count; ++i) {
-        pa_params q = prms[i];
-        q.tile_passes = P;   // one pass count per launch
-        const int rc = make_plan(&q, &L.plans[i]);
-        if (rc != PA_OK) return rc;
-        const GenPlan &p = L.plans[i];
-        if (prms[i].id_bits != prms[0].id_bits) return PA_ERR_INVALID;
-        if (prms[i].n + p.tile_nodes + 32 >= (1ull << 32)) return PA_ERR_NOT_SUPPORTED;
-        if (prms[i].flags != 0) return PA_ERR_INVALID;
-        sb[i] = level_bounds(p.u_first, p.u_first, p.u_split, (uint64_t)kStartPasses * p.groups);
-        tb[i] = level_bounds(p.u_first, p.u_split, prms[i].n, p.tile_nodes);
-        L.max_start_pairs = std::max<uint64_t>(L.max_start_pairs, (p.u_split - p.u_first) * prms[i].d);
-    }
-    build_levels(sb, L.start);
-    build_levels(tb, L.tail);
-    if (L.start.levels > kMaxLevels || L.tail.levels > kMaxLevels) return PA_ERR_NOT_SUPPORTED;
-    uint64_t o = kCtlBytes;
-    L.table_off = o;
-    o += al((uint64_t)count * sizeof(GenArgs));
-    for (HostLevels *H : {&L.start, &L.tail}) {
-        H->lvl_off = o;
-        o += al(8ull * H->lvl.size());
-        H->ibase_off = o;
-        o += al(8ull * H->ibase.size());
-        H->lstart_off = o;
-        o += al(8ull * H->lstart.size());
-    }
-    L.ticket_off = o;
-    o += 256;
-    L.inst_off = o;
-    for (uint32_t i = 0; i < count; ++i) {
-        L.flags_off[i] = o;
-        o += al(4 * L.plans[i].n_tiles);
-        L.sb_off[i] = o;
-        o += al(4 * L.plans[i].n_sb);
-    }
-    L.total = o;
-    return PA_OK;
-}
-
-gen::LevelTables device_tables(const HostLevels &H, unsigned char *scr)
+gen::LevelTables device_tables(const BatchLevels &H, unsigned char *scr)
 {
     gen::LevelTables t;
     t.lvl_base = reinterpret_cast<const unsigned long long *>(scr + H.lvl_off);
@@ -290,47 +221,82 @@ gen::LevelTables device_tables(const HostLevels &H, unsigned char *scr)
 }
 
 }  // namespace
-}  // namespace pa
 
-using namespace pa;
-
-extern "C" {
-
-int pa_batch_scratch_bytes(const pa_params *prms, uint32_t count, uint64_t *bytes)
+int batch_prepare(const pa_params *prms, uint32_t count, BatchJob &J)
 {
-    if (!bytes) return PA_ERR_INVALID;
-    BatchLayout L;
-    const int rc = batch_layout(prms, count, L);
-    if (rc != PA_OK) return rc;
-    *bytes = L.total;
+    if (!prms || count == 0) return PA_ERR_INVALID;
+    auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
+    // one pass per tile by default: small tiles keep the dependency chains short
+    const uint32_t P = prms[0].tile_passes ? prms[0].tile_passes : 1u;
+    if (P != 1 && P != 2 && P != 4) return PA_ERR_NOT_SUPPORTED;
+    J.count = count;
+    J.passes = P;
+    J.id_bytes = prms[0].id_bits / 8;
+    J.plans.assign(count, GenPlan{});
+    J.flags_off.assign(count, 0);
+    J.sb_off.assign(count, 0);
+    J.max_start_pairs = 0;
+    std::vector<std::vector<uint64_t>> sb(count), tb(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        pa_params q = prms[i];
+        q.tile_passes = P;   // one pass count per launch
+        const int rc = make_plan(&q, &J.plans[i]);
+        if (rc != PA_OK) return rc;
+        const GenPlan &p = J.plans[i];
+        if (prms[i].id_bits != prms[0].id_bits) return PA_ERR_INVALID;
+        if (prms[i].n + p.tile_nodes + 32 >= (1ull << 32)) return PA_ERR_NOT_SUPPORTED;
+        if (prms[i].flags != 0) return PA_ERR_INVALID;
+        sb[i] = level_bounds(p.u_first, p.u_first, p.u_split, (uint64_t)kStartPasses * p.groups);
+        tb[i] = level_bounds(p.u_first, p.u_split, prms[i].n, p.tile_nodes);
+        J.max_start_pairs = std::max<uint64_t>(J.max_start_pairs, (p.u_split - p.u_first) * prms[i].d);
+    }
+    build_levels(sb, J.start);
+    build_levels(tb, J.tail);
+    if (J.start.levels > kMaxLevels || J.tail.levels > kMaxLevels) return PA_ERR_NOT_SUPPORTED;
+    // scratch: control block | image (GenArgs table, level tables) | tickets, flags, counts
+    uint64_t o = kCtlBytes;
+    J.image_off = o;
+    J.table_off = o;
+    o += al((uint64_t)count * sizeof(gen::GenArgs));
+    for (BatchLevels *H : {&J.start, &J.tail}) {
+        H->lvl_off = o;
+        o += al(8ull * H->lvl.size());
+        H->ibase_off = o;
+        o += al(8ull * H->ibase.size());
+        H->lstart_off = o;
+        o += al(8ull * H->lstart.size());
+    }
+    J.image_bytes = o - J.image_off;
+    J.ticket_off = o;
+    o += 256;
+    for (uint32_t i = 0; i < count; ++i) {
+        J.flags_off[i] = o;
+        o += al(4 * J.plans[i].n_tiles);
+        J.sb_off[i] = o;
+        o += al(4 * J.plans[i].n_sb);
+    }
+    J.scratch_bytes = o;
     return PA_OK;
 }
 
-int pa_batch_generate(const pa_params *prms, uint32_t count, void *const *d_edges,
-                      const uint64_t *edges_bytes, void *d_scratch, uint64_t scratch_bytes,
-                      void *stream)
+int batch_bind(BatchJob &J, const pa_params *prms, void *const *d_edges, const uint64_t *edges_bytes,
+               void *d_scratch, unsigned char *image)
 {
-    BatchLayout L;
-    int rc = batch_layout(prms, count, L);
-    if (rc != PA_OK) return rc;
-    if (!d_edges || !edges_bytes || !d_scratch) return PA_ERR_INVALID;
-    if (scratch_bytes < L.total) return PA_ERR_CAPACITY;
+    if (!d_edges || !edges_bytes || !d_scratch || !image) return PA_ERR_INVALID;
     if (reinterpret_cast<uintptr_t>(d_scratch) & 15u) return PA_ERR_INVALID;
-    const uint32_t P = batch_passes(prms);
-    if (P != 1 && P != 2 && P != 4) return PA_ERR_NOT_SUPPORTED;
     unsigned char *scr = (unsigned char *)d_scratch;
-    std::vector<gen::GenArgs> table(count);
-    for (uint32_t i = 0; i < count; ++i) {
-        const GenPlan &p = L.plans[i];
+    gen::GenArgs *table = reinterpret_cast<gen::GenArgs *>(image + (J.table_off - J.image_off));
+    for (uint32_t i = 0; i < J.count; ++i) {
+        const GenPlan &p = J.plans[i];
         if (!d_edges[i] || (reinterpret_cast<uintptr_t>(d_edges[i]) & 15u)) return PA_ERR_INVALID;
         if (edges_bytes[i] < p.edges_bytes) return PA_ERR_CAPACITY;
-        gen::GenArgs &a = table[i];
+        gen::GenArgs a;
         std::memset(&a, 0, sizeof(a));
         a.edges = d_edges[i];
         a.ctl = reinterpret_cast<GenCtl *>(scr);
         a.reps = reinterpret_cast<GenRep *>(scr + kRepOffset);
-        a.flags = reinterpret_cast<uint32_t *>(scr + L.flags_off[i]);
-        a.sbcnt = reinterpret_cast<uint32_t *>(scr + L.sb_off[i]);
+        a.flags = reinterpret_cast<uint32_t *>(scr + J.flags_off[i]);
+        a.sbcnt = reinterpret_cast<uint32_t *>(scr + J.sb_off[i]);
         a.n_sb = p.n_sb;
         a.sb_nodes = (uint64_t)kSbTiles * p.tile_nodes;
         a.n = prms[i].n;
@@ -350,48 +316,79 @@ int pa_batch_generate(const pa_params *prms, uint32_t count, void *const *d_edge
         a.window_shift = 63;
         a.min_window = 0;
         a.start_end = p.u_split;
+        std::memcpy(table + i, &a, sizeof(a));
+        if (i == 0) J.first = a;
     }
-    cudaStream_t s = (cudaStream_t)stream;
-    cudaError_t e = cudaMemsetAsync(scr, 0, kCtlBytes, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(scr + L.ticket_off, 0, L.total - L.ticket_off, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(scr + L.table_off, table.data(), count * sizeof(gen::GenArgs),
-                            cudaMemcpyHostToDevice, s);
-    for (const HostLevels *H : {&L.start, &L.tail}) {
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(scr + H->lvl_off, H->lvl.data(), H->lvl.size() * 8ull,
-                                cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(scr + H->ibase_off, H->ibase.data(), H->ibase.size() * 8ull,
-                                cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(scr + H->lstart_off, H->lstart.data(), H->lstart.size() * 8ull,
-                                cudaMemcpyHostToDevice, s);
+    for (const BatchLevels *H : {&J.start, &J.tail}) {
+        std::memcpy(image + (H->lvl_off - J.image_off), H->lvl.data(), H->lvl.size() * 8ull);
+        std::memcpy(image + (H->ibase_off - J.image_off), H->ibase.data(), H->ibase.size() * 8ull);
+        std::memcpy(image + (H->lstart_off - J.image_off), H->lstart.data(), H->lstart.size() * 8ull);
     }
-    // the host vectors are pageable: make sure the copies have read them
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return set_cuda_error(e);
+    return PA_OK;
+}
 
-    const gen::GenArgs *d_inst = reinterpret_cast<const gen::GenArgs *>(scr + L.table_off);
-    unsigned long long *tickets = reinterpret_cast<unsigned long long *>(scr + L.ticket_off);
+int batch_enqueue(const BatchJob &J, void *d_scratch, const void *image, cudaStream_t s)
+{
+    unsigned char *scr = (unsigned char *)d_scratch;
+    cudaError_t e = cudaMemsetAsync(scr, 0, kCtlBytes, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(scr + J.ticket_off, 0, J.scratch_bytes - J.ticket_off, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(scr + J.image_off, image, J.image_bytes, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    const gen::GenArgs *d_inst = reinterpret_cast<const gen::GenArgs *>(scr + J.table_off);
+    unsigned long long *tickets = reinterpret_cast<unsigned long long *>(scr + J.ticket_off);
     GenCtl *ctl = reinterpret_cast<GenCtl *>(scr);
-    const uint32_t id_bytes = prms[0].id_bits / 8;
-    rc = gen::fill_start(id_bytes, d_inst, count, L.max_start_pairs, s);
+    int rc = gen::fill_start(J.id_bytes, d_inst, J.count, J.max_start_pairs, s);
     if (rc != PA_OK) return rc;
     gen::StartArgs sa;
     std::memset(&sa, 0, sizeof(sa));
     sa.inst = d_inst;
-    sa.tab = device_tables(L.start, scr);
-    sa.count = count;
+    sa.tab = device_tables(J.start, scr);
+    sa.count = J.count;
     sa.write_seeds = 1;
-    sa.t_end = L.start.lvl[L.start.levels];
+    sa.t_end = J.start.lvl[J.start.levels];
     sa.ticket = tickets;
     sa.ctl = ctl;
-    if (count == 1) sa.one = table[0];
-    rc = gen::launch_start(id_bytes, sa, 0, s);
+    if (J.count == 1) sa.one = J.first;
+    rc = gen::launch_start(J.id_bytes, sa, 0, s);
     if (rc != PA_OK) return rc;
-    return gen::launch_tail(id_bytes, P, d_inst, device_tables(L.tail, scr), count,
-                            L.tail.lvl[0], L.tail.lvl[L.tail.levels], tickets + 1, ctl, s);
+    return gen::launch_tail(J.id_bytes, J.passes, d_inst, device_tables(J.tail, scr), J.count,
+                            J.tail.lvl[0], J.tail.lvl[J.tail.levels], tickets + 1, ctl, s);
+}
+
+}  // namespace pa
+
+using namespace pa;
+
+extern "C" {
+
+int pa_batch_scratch_bytes(const pa_params *prms, uint32_t count, uint64_t *bytes)
+{
+    if (!bytes) return PA_ERR_INVALID;
+    BatchJob J;
+    const int rc = batch_prepare(prms, count, J);
+    if (rc != PA_OK) return rc;
+    *bytes = J.scratch_bytes;
+    return PA_OK;
+}
+
+int pa_batch_generate(const pa_params *prms, uint32_t count, void *const *d_edges,
+                      const uint64_t *edges_bytes, void *d_scratch, uint64_t scratch_bytes,
+                      void *stream)
+{
+    BatchJob J;
+    int rc = batch_prepare(prms, count, J);
+    if (rc != PA_OK) return rc;
+    if (scratch_bytes < J.scratch_bytes) return PA_ERR_CAPACITY;
+    std::vector<unsigned char> image(J.image_bytes);
+    rc = batch_bind(J, prms, d_edges, edges_bytes, d_scratch, image.data());
+    if (rc != PA_OK) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    rc = batch_enqueue(J, d_scratch, image.data(), s);
+    if (rc != PA_OK) return rc;
+    // the image is pageable host memory: make sure the copy has read it
+    const cudaError_t e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? PA_OK : set_cuda_error(e);
 }
 
 }  // extern "C"

@@ -103,6 +103,40 @@ class PaGraph(ctypes.Structure):
     ]
 
 
+class PaServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("budget_bytes", ctypes.c_uint64),
+        ("max_batch", ctypes.c_uint32),
+        ("max_inflight", ctypes.c_uint32),
+        ("max_queue", ctypes.c_uint32),
+        ("device", ctypes.c_int32),
+        ("ttl_ns", ctypes.c_uint64),
+        ("aging_ns", ctypes.c_uint64),
+    ]
+
+
+class PaResult(ctypes.Structure):
+    _fields_ = [
+        ("edges", ctypes.c_void_p),
+        ("n_edges", ctypes.c_uint64),
+        ("edges_bytes", ctypes.c_uint64),
+        ("status", ctypes.c_int32),
+        ("batch_size", ctypes.c_uint32),
+        ("t_submit_ns", ctypes.c_uint64),
+        ("t_start_ns", ctypes.c_uint64),
+        ("t_done_ns", ctypes.c_uint64),
+    ]
+
+
+class PaServerStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint64) for k in (
+        "submitted", "completed", "released", "expired", "failed", "batches", "queued",
+        "running", "bytes_in_use", "budget_bytes", "edges_done")]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib: Optional[ctypes.CDLL] = None
 
 _P = ctypes.POINTER
@@ -142,6 +176,24 @@ _SIGS = {
     "pa_graph_create": (ctypes.c_int, [_P(PaParams), _P(PaGraph)]),
     "pa_graph_generate": (ctypes.c_int, [_P(PaGraph), ctypes.c_void_p, _P(PaStats)]),
     "pa_graph_destroy": (ctypes.c_int, [_P(PaGraph)]),
+    "pa_server_config_init": (ctypes.c_int, [_P(PaServerConfig)]),
+    "pa_server_create": (ctypes.c_int, [_P(PaServerConfig), _P(ctypes.c_void_p)]),
+    "pa_server_submit": (ctypes.c_int, [ctypes.c_void_p, _P(PaParams), _P(ctypes.c_uint64)]),
+    "pa_server_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _P(PaResult)]),
+    "pa_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                      _P(PaResult)]),
+    "pa_server_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    "pa_server_stats_get": (ctypes.c_int, [ctypes.c_void_p, _P(PaServerStats)]),
+    "pa_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "pa_sched_create": (ctypes.c_void_p, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32]),
+    "pa_sched_destroy": (None, [ctypes.c_void_p]),
+    "pa_sched_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                       ctypes.c_uint64]),
+    "pa_sched_admit": (ctypes.c_uint32, [ctypes.c_void_p, ctypes.c_uint64, _P(ctypes.c_uint64),
+                                         ctypes.c_uint32]),
+    "pa_sched_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64]),
+    "pa_sched_in_use": (ctypes.c_uint64, [ctypes.c_void_p]),
+    "pa_sched_queued": (ctypes.c_uint64, [ctypes.c_void_p]),
 }
 
 
@@ -412,3 +464,116 @@ class cuPPA:  # noqa: N801 - reference class name
         write_degree_distribution(self._prm, self.edges, path)
         with open(path) as f:
             return f.read()
+
+
+# ---------------------------------------------------------------------------
+# Request server and its admission queue
+# ---------------------------------------------------------------------------
+class _DeviceArray:
+    """A device buffer the server owns, exposed through __cuda_array_interface__
+    so torch.as_tensor can view it without a copy."""
+
+    def __init__(self, ptr: int, shape, typestr: str):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr,
+                                         "data": (ptr, False), "version": 2, "strides": None}
+
+
+class Sched:
+    """The server's admission queue alone (host logic; no GPU needed)."""
+
+    def __init__(self, budget_bytes: int, aging_ns: int = 100_000_000, max_queue: int = 0):
+        self._h = lib().pa_sched_create(budget_bytes, aging_ns, max_queue)
+        if not self._h:
+            raise MemoryError("pa_sched_create")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pa_sched_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def submit(self, ticket: int, nbytes: int, now_ns: int) -> int:
+        return lib().pa_sched_submit(self._h, ticket, nbytes, now_ns)
+
+    def admit(self, now_ns: int, cap: int = 4096) -> list:
+        out = (ctypes.c_uint64 * cap)()
+        n = lib().pa_sched_admit(self._h, now_ns, out, cap)
+        return [int(out[i]) for i in range(n)]
+
+    def release(self, ticket: int, nbytes: int = (1 << 64) - 1) -> int:
+        return lib().pa_sched_release(self._h, ticket, nbytes)
+
+    @property
+    def in_use(self) -> int:
+        return int(lib().pa_sched_in_use(self._h))
+
+    @property
+    def queued(self) -> int:
+        return int(lib().pa_sched_queued(self._h))
+
+
+class Server:
+    """Continuous-batching generation server (pa_server_*)."""
+
+    def __init__(self, budget_bytes: int = 0, max_batch: int = 0, max_inflight: int = 0,
+                 max_queue: int = 0, device: int = -1, ttl_ns: int = 0, aging_ns: int = 0):
+        cfg = PaServerConfig()
+        check(lib().pa_server_config_init(ctypes.byref(cfg)), "pa_server_config_init")
+        cfg.budget_bytes, cfg.max_batch, cfg.max_inflight = budget_bytes, max_batch, max_inflight
+        cfg.max_queue, cfg.device, cfg.ttl_ns, cfg.aging_ns = max_queue, device, ttl_ns, aging_ns
+        h = ctypes.c_void_p()
+        check(lib().pa_server_create(ctypes.byref(cfg), ctypes.byref(h)), "pa_server_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pa_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, prm: PaParams) -> int:
+        t = ctypes.c_uint64()
+        check(lib().pa_server_submit(self._h, ctypes.byref(prm), ctypes.byref(t)),
+              "pa_server_submit")
+        return int(t.value)
+
+    def try_submit(self, prm: PaParams):
+        """(status, ticket) without raising."""
+        t = ctypes.c_uint64()
+        rc = lib().pa_server_submit(self._h, ctypes.byref(prm), ctypes.byref(t))
+        return rc, int(t.value)
+
+    def poll(self, ticket: int):
+        """(status, PaResult): PA_OK when finished, PA_ERR_BUSY while pending."""
+        r = PaResult()
+        rc = lib().pa_server_poll(self._h, ticket, ctypes.byref(r))
+        return rc, r
+
+    def wait(self, ticket: int, timeout_ns: int = 0):
+        r = PaResult()
+        rc = lib().pa_server_wait(self._h, ticket, timeout_ns, ctypes.byref(r))
+        return rc, r
+
+    def release(self, ticket: int) -> int:
+        return lib().pa_server_release(self._h, ticket)
+
+    def stats(self) -> PaServerStats:
+        st = PaServerStats()
+        check(lib().pa_server_stats_get(self._h, ctypes.byref(st)), "pa_server_stats_get")
+        return st
+
+    @staticmethod
+    def edges_view(result: PaResult, id_bits: int):
+        """A torch tensor [n_edges, 2] viewing a finished result's device buffer
+        (valid until the ticket is released)."""
+        torch = _torch()
+        ts = "<i8" if id_bits == 64 else "<i4"
+        arr = _DeviceArray(int(result.edges), (int(result.n_edges), 2), ts)
+        return torch.as_tensor(arr, device="cuda")
+

@@ -163,18 +163,107 @@ int pa_build_csr(const pa_params *prm, const void *d_edges, int64_t *d_rowptr, v
                  void *d_scratch, uint64_t scratch_bytes, void *stream);
 
 /* ---- batches ---------------------------------------------------------------- */
-/* Many independent graphs in one persistent launch (no counterpart in the
- * reference, which makes one graph per run).  prms[i] describes graph i (all of
- * one id width, every n < 2^32 - 64; tile_passes is taken from prms[0]); graph i
- * is written to d_edges[i] (edges_bytes[i] >= pa_edges_bytes(prms[i])) exactly as
- * pa_generate would write it.  The graphs' tiles are claimed in the order given:
- * list large graphs first.  The call copies a small table to the device and
- * waits for that copy, then returns with the launch queued; read the status with
- * pa_generate_finish(d_scratch, ...). */
+/* Many independent graphs in shared launches (no counterpart in the reference,
+ * which makes one graph per run): one fill, one start-kernel launch over every
+ * graph's start region and one tail launch over the rest, the work of all
+ * graphs interleaved level by level.  prms[i] describes graph i (all of one id
+ * width, every n < 2^32 - 64; tile_passes is taken from prms[0]); graph i is
+ * written to d_edges[i] (edges_bytes[i] >= pa_edges_bytes(prms[i])) exactly as
+ * pa_generate would write it.  The call copies a small table to the device and
+ * waits for that copy, then returns with the launches queued; read the status
+ * with pa_generate_finish(d_scratch, ...). */
 int pa_batch_scratch_bytes(const pa_params *prms, uint32_t count, uint64_t *bytes);
 int pa_batch_generate(const pa_params *prms, uint32_t count, void *const *d_edges,
                       const uint64_t *edges_bytes, void *d_scratch, uint64_t scratch_bytes,
                       void *stream);
+
+/* ---- request server ------------------------------------------------------------ */
+/* A served stream of independent generation requests (no counterpart in the
+ * reference, which makes one graph per process run, src/main.cu:105-116).  One
+ * control thread per server owns a CUDA stream on its device: it admits queued
+ * requests while their device memory (edge buffer + generation scratch) fits
+ * the budget, launches everything admitted as one batch (pa_batch_generate's
+ * launches) whenever fewer than max_inflight batches are on the GPU -- so
+ * requests that arrive while a batch runs form the next one -- and marks each
+ * request done when its batch's completion event has fired.  A result stays in
+ * device memory, owned by the server, until pa_server_release (or until it has
+ * been finished for ttl_ns).  Submit, poll, wait and release may be called from
+ * any thread. */
+typedef struct pa_server pa_server;
+
+typedef struct pa_server_config {
+    uint64_t budget_bytes;   /* device memory for admitted requests; 0 = 3/4 of free memory */
+    uint32_t max_batch;      /* requests per launch; 0 = 4096                              */
+    uint32_t max_inflight;   /* batches queued on the GPU at once; 0 = 2                   */
+    uint32_t max_queue;      /* queued (not yet admitted) requests; 0 = unlimited          */
+    int32_t device;          /* CUDA device; -1 = the caller's current device              */
+    uint64_t ttl_ns;         /* finished results unreleased this long are freed; 0 = never */
+    uint64_t aging_ns;       /* a queued request that has waited this long is not passed
+                                over by smaller ones; 0 = 100 ms                           */
+} pa_server_config;
+
+typedef struct pa_result {
+    const void *edges;       /* device pointer (the PAIRS layout), valid until release   */
+    uint64_t n_edges;
+    uint64_t edges_bytes;
+    int32_t status;          /* pa_status of the generation                              */
+    uint32_t batch_size;     /* requests in the launch that produced it                  */
+    uint64_t t_submit_ns;    /* server clock: ns since pa_server_create                   */
+    uint64_t t_start_ns;     /* its batch was launched                                    */
+    uint64_t t_done_ns;      /* the control thread saw the batch complete                 */
+} pa_result;
+
+typedef struct pa_server_stats {
+    uint64_t submitted, completed, released, expired, failed;
+    uint64_t batches;        /* launches so far                                           */
+    uint64_t queued;         /* waiting for admission now                                 */
+    uint64_t running;        /* admitted, not finished                                    */
+    uint64_t bytes_in_use;   /* budget held by admitted and unreleased requests           */
+    uint64_t budget_bytes;
+    uint64_t edges_done;     /* edges of completed requests                               */
+} pa_server_stats;
+
+int pa_server_config_init(pa_server_config *cfg);
+/* Start a server (its control thread and stream); *out gets the handle. */
+int pa_server_create(const pa_server_config *cfg, pa_server **out);
+/* Queue a request (a copy of *prm is kept; id widths may differ between
+ * requests).  PA_ERR_CAPACITY: it can never fit the budget; PA_ERR_BUSY: the
+ * queue is full.  *ticket identifies it from then on. */
+int pa_server_submit(pa_server *srv, const pa_params *prm, uint64_t *ticket);
+/* PA_OK with *out filled once the request is finished (its own outcome in
+ * out->status), PA_ERR_BUSY while it is queued or running, PA_ERR_NOT_FOUND for
+ * an unknown, released or expired ticket. */
+int pa_server_poll(pa_server *srv, uint64_t ticket, pa_result *out);
+/* As poll, but blocks up to timeout_ns (0 = no limit) for the request to finish. */
+int pa_server_wait(pa_server *srv, uint64_t ticket, uint64_t timeout_ns, pa_result *out);
+/* Give a finished (or still queued) request's memory back to the budget;
+ * PA_ERR_BUSY while it runs.  The caller's own reads of the result must have
+ * completed. */
+int pa_server_release(pa_server *srv, uint64_t ticket);
+int pa_server_stats_get(pa_server *srv, pa_server_stats *out);
+/* Stop the control thread, wait for the GPU work, free everything.  No other
+ * thread may be inside a pa_server_* call on this handle. */
+int pa_server_destroy(pa_server *srv);
+
+/* The server's admission queue on its own (host logic, no GPU), for tests and
+ * for callers that schedule their own launches.  Arrival order is kept: a
+ * request whose bytes fit the free budget is admitted; one that does not is
+ * passed over, unless it has waited aging_ns, which stops the scan so that a
+ * large request is not starved by a stream of small ones. */
+typedef struct pa_sched pa_sched;
+pa_sched *pa_sched_create(uint64_t budget_bytes, uint64_t aging_ns, uint32_t max_queue);
+void pa_sched_destroy(pa_sched *q);
+/* PA_OK, PA_ERR_CAPACITY (bytes > budget), PA_ERR_BUSY (queue full),
+ * PA_ERR_INVALID (ticket already known). */
+int pa_sched_submit(pa_sched *q, uint64_t ticket, uint64_t bytes, uint64_t now_ns);
+/* Admit up to cap requests; their tickets go to out[], the count is returned. */
+uint32_t pa_sched_admit(pa_sched *q, uint64_t now_ns, uint64_t *out, uint32_t cap);
+/* Return `bytes` of an admitted request to the budget (all of them when bytes
+ * is UINT64_MAX, which also forgets the ticket; a queued request is withdrawn).
+ * PA_ERR_NOT_FOUND if unknown. */
+int pa_sched_release(pa_sched *q, uint64_t ticket, uint64_t bytes);
+uint64_t pa_sched_in_use(const pa_sched *q);
+uint64_t pa_sched_queued(const pa_sched *q);
 
 /* ---- files ------------------------------------------------------------------ */
 enum { PA_FORMAT_TEXT = 0, PA_FORMAT_BINARY = 1 };

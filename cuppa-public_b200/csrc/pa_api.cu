@@ -150,6 +150,16 @@ int pa_edges_bytes(const pa_params *prm, uint64_t *bytes)
     return PA_OK;
 }
 
+int pa_start_split(const pa_params *prm, uint64_t *u_split)
+{
+    GenPlan p;
+    const int rc = make_plan(prm, &p);
+    if (rc != PA_OK) return rc;
+    if (!u_split) return PA_ERR_INVALID;
+    *u_split = p.u_split;
+    return PA_OK;
+}
+
 int pa_scratch_bytes(const pa_params *prm, uint64_t *bytes)
 {
     GenPlan p;
@@ -171,6 +181,21 @@ int pa_generate(const pa_params *prm, void *d_edges, uint64_t edges_bytes, void 
         return PA_ERR_INVALID;
     if (edges_bytes < p.edges_bytes || scratch_bytes < p.scratch_bytes) return PA_ERR_CAPACITY;
     return launch_generate(prm, p, d_edges, d_scratch, (cudaStream_t)stream, 0);
+}
+
+int pa_generate_timed(const pa_params *prm, void *d_edges, uint64_t edges_bytes, void *d_scratch,
+                      uint64_t scratch_bytes, void *stream, void *const *events)
+{
+    GenPlan p;
+    const int rc = make_plan(prm, &p);
+    if (rc != PA_OK) return rc;
+    if (!d_edges || !d_scratch || !events) return PA_ERR_INVALID;
+    if ((reinterpret_cast<uintptr_t>(d_edges) & 15u) || (reinterpret_cast<uintptr_t>(d_scratch) & 15u))
+        return PA_ERR_INVALID;
+    if (edges_bytes < p.edges_bytes || scratch_bytes < p.scratch_bytes) return PA_ERR_CAPACITY;
+    const cudaEvent_t ev[3] = {(cudaEvent_t)events[0], (cudaEvent_t)events[1],
+                               (cudaEvent_t)events[2]};
+    return launch_generate(prm, p, d_edges, d_scratch, (cudaStream_t)stream, 0, ev);
 }
 
 int pa_generate_finish(const void *d_scratch, pa_stats *out, void *stream)

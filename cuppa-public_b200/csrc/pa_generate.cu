@@ -358,8 +358,17 @@ int launch_passes(const GenArgs &a, uint32_t passes, uint32_t blocks, cudaStream
 }  // namespace
 
 int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, void *d_scratch,
-                    cudaStream_t stream, uint32_t blocks_override)
+                    cudaStream_t stream, uint32_t blocks_override, const cudaEvent_t *events)
 {
+    // optional phase marks: [0] before the first launch, [1] between the start
+    // region and the persistent launch, [2] after the last launch
+    auto mark = [&](int i) -> int {
+        if (!events || !events[i]) return PA_OK;
+        const cudaError_t er = cudaEventRecord(events[i], stream);
+        return er == cudaSuccess ? PA_OK : set_cuda_error(er);
+    };
+    int mrc = mark(0);
+    if (mrc != PA_OK) return mrc;
     cudaError_t e = cudaMemsetAsync(d_scratch, 0, plan.scratch_bytes, stream);
     if (e != cudaSuccess) return set_cuda_error(e);
 
@@ -419,15 +428,23 @@ int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, vo
         sa.ctl = a.ctl;
         const int rc = launch_start(plan.id_bytes, sa, blocks, stream);
         if (rc != PA_OK) return rc;
-        if (plan.u_split >= prm->n) return PA_OK;
+        if (plan.u_split >= prm->n) {
+            mrc = mark(1);
+            return mrc != PA_OK ? mrc : mark(2);
+        }
         // u_split - u_first is a whole number of superblocks
         a.tile_begin = (plan.u_split - plan.u_first) / plan.tile_nodes;
         a.water_init = a.tile_begin / kSbTiles;
     }
+    mrc = mark(1);
+    if (mrc != PA_OK) return mrc;
+    int rc;
     if (plan.id_bytes == 8)
-        return small ? launch_passes<int64_t, uint32_t>(a, plan.passes, blocks, stream)
-                     : launch_passes<int64_t, uint64_t>(a, plan.passes, blocks, stream);
-    return launch_passes<int32_t, uint32_t>(a, plan.passes, blocks, stream);
+        rc = small ? launch_passes<int64_t, uint32_t>(a, plan.passes, blocks, stream)
+                   : launch_passes<int64_t, uint64_t>(a, plan.passes, blocks, stream);
+    else
+        rc = launch_passes<int32_t, uint32_t>(a, plan.passes, blocks, stream);
+    return rc != PA_OK ? rc : mark(2);
 }
 
 }  // namespace pa

@@ -79,6 +79,7 @@ constexpr uint64_t kStartNodesAuto = 1ull << 24;
 // Launch the generator kernel on `stream` into caller memory; scratch must hold
 // plan.scratch_bytes and is cleared here.
 int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, void *d_scratch,
-                    cudaStream_t stream, uint32_t blocks_override);
+                    cudaStream_t stream, uint32_t blocks_override,
+                    const cudaEvent_t *events = nullptr);
 
 }  // namespace pa

@@ -161,8 +161,24 @@ void launch_group(pa_server *S, const std::vector<uint64_t> &tickets,
     L.tickets = tickets;
     int rc = PA_OK;
     cudaError_t e = cudaSuccess;
-    for (uint32_t i = 0; i < k && e == cudaSuccess; ++i)
-        e = cudaMallocFromPoolAsync(&edges[i], std::max<uint64_t>(ebytes[i], 16), S->pool, S->stream);
+    // The budget bounds what is held, but the pool's free blocks can be too
+    // fragmented for a large buffer: on failure, give the pool's unused memory
+    // back to the device and try once more.
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        e = cudaSuccess;
+        for (uint32_t i = 0; i < k && e == cudaSuccess; ++i)
+            e = cudaMallocFromPoolAsync(&edges[i], std::max<uint64_t>(ebytes[i], 16), S->pool,
+                                        S->stream);
+        if (e == cudaSuccess || attempt == 1) break;
+        (void)cudaGetLastError();
+        for (uint32_t i = 0; i < k; ++i)
+            if (edges[i]) {
+                cudaFreeAsync(edges[i], S->stream);
+                edges[i] = nullptr;
+            }
+        cudaStreamSynchronize(S->stream);
+        cudaMemPoolTrimTo(S->pool, 0);
+    }
     if (e != cudaSuccess) rc = set_cuda_error(e);
     BatchJob J;
     uint64_t scratch_bytes = 0, image_bytes = 0;
@@ -177,6 +193,12 @@ void launch_group(pa_server *S, const std::vector<uint64_t> &tickets,
     }
     if (rc == PA_OK) {
         e = cudaMallocFromPoolAsync(&L.scratch, scratch_bytes, S->pool, S->stream);
+        if (e != cudaSuccess) {
+            (void)cudaGetLastError();
+            cudaStreamSynchronize(S->stream);
+            cudaMemPoolTrimTo(S->pool, 0);
+            e = cudaMallocFromPoolAsync(&L.scratch, scratch_bytes, S->pool, S->stream);
+        }
         if (e != cudaSuccess) rc = set_cuda_error(e);
     }
     if (rc == PA_OK) {

@@ -153,6 +153,10 @@ _SIGS = {
     "pa_generate": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_uint64,
                                    ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),
     "pa_generate_finish": (ctypes.c_int, [ctypes.c_void_p, _P(PaStats), ctypes.c_void_p]),
+    "pa_start_split": (ctypes.c_int, [_P(PaParams), _P(ctypes.c_uint64)]),
+    "pa_generate_timed": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_uint64,
+                                         ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                         _P(ctypes.c_void_p)]),
     "pa_generate_trace": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_void_p,
                                          ctypes.c_uint32, _P(ctypes.c_uint32), ctypes.c_void_p]),
     "pa_canonicalize": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_void_p,
@@ -281,6 +285,28 @@ def generate_into(prm: PaParams, edges, scratch, stream=None) -> None:
                            ctypes.c_void_p(scratch.data_ptr()), scratch.numel(),
                            ctypes.c_void_p(_stream_ptr(stream)))
     check(rc, "pa_generate")
+
+
+def generate_timed(prm: PaParams, edges, scratch, events, stream=None) -> None:
+    """pa_generate_timed: `events` are three torch.cuda.Event(enable_timing=True)
+    recorded before the first launch, between the start region and the
+    persistent launch, and after the last launch."""
+    for ev in events:
+        if not ev.cuda_event:
+            ev.record(stream)      # the CUDA event is created on first record
+    arr = (ctypes.c_void_p * 3)(*[ev.cuda_event for ev in events])
+    rc = lib().pa_generate_timed(ctypes.byref(prm), ctypes.c_void_p(edges.data_ptr()),
+                                 edges.numel() * edges.element_size(),
+                                 ctypes.c_void_p(scratch.data_ptr()), scratch.numel(),
+                                 ctypes.c_void_p(_stream_ptr(stream)), arr)
+    check(rc, "pa_generate_timed")
+
+
+def start_split(prm: PaParams) -> int:
+    """First node left to the persistent launch (pa_start_split)."""
+    u = ctypes.c_uint64()
+    check(lib().pa_start_split(ctypes.byref(prm), ctypes.byref(u)), "pa_start_split")
+    return int(u.value)
 
 
 def finish(scratch, stream=None) -> PaStats:

@@ -106,12 +106,24 @@ uint64_t pa_edge_count(const pa_params *prm);
 int pa_edges_bytes(const pa_params *prm, uint64_t *bytes);
 int pa_scratch_bytes(const pa_params *prm, uint64_t *bytes);
 
+/* Nodes [d+1, *u_split) are generated by the start kernel (pa_params.start_nodes
+ * rounded up to whole superblocks of the persistent launch, at most n); the
+ * rest by the persistent launch. */
+int pa_start_split(const pa_params *prm, uint64_t *u_split);
+
 /* ---- generation ---------------------------------------------------------- */
 /* Stream-ordered generation into caller memory.  d_scratch (pa_scratch_bytes)
  * is cleared by the call; it must not be shared by generations that overlap.
  * Host-side errors return at once; device-side status is read by pa_generate_finish. */
 int pa_generate(const pa_params *prm, void *d_edges, uint64_t edges_bytes, void *d_scratch,
                 uint64_t scratch_bytes, void *stream);
+/* pa_generate with the phases timed: events[0..2] (cudaEvent_t, any may be
+ * NULL) are recorded on `stream` before the first launch, between the start
+ * kernel's region and the persistent launch, and after the last launch.  The
+ * device side of the per-stage timing table the reference writes
+ * (src/PA/cuPPA/cuPPA_1.cu:84-87,217-223). */
+int pa_generate_timed(const pa_params *prm, void *d_edges, uint64_t edges_bytes, void *d_scratch,
+                      uint64_t scratch_bytes, void *stream, void *const *events);
 /* Wait for the stream, then copy the status and counters of the generation that
  * last used d_scratch.  Returns the device status. */
 int pa_generate_finish(const void *d_scratch, pa_stats *out, void *stream);

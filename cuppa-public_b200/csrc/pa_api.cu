@@ -59,12 +59,15 @@ int make_plan(const pa_params *prm, GenPlan *plan)
     p.sb_offset = kCtlBytes + ((p.n_tiles * 4ull + 255ull) & ~255ull);
     p.trace_offset = p.sb_offset + ((p.n_sb * 4ull + 255ull) & ~255ull);
     p.start_offset = p.trace_offset + (uint64_t)kTraceMax * 16ull;
-    p.scratch_bytes = p.start_offset + kStartAreaBytes;
     p.spin_limit_ns = prm->spin_limit_ns ? prm->spin_limit_ns : 2000000000ull;
     const uint64_t want = prm->start_nodes == PA_START_NONE ? 0
                           : prm->start_nodes ? prm->start_nodes
                                              : kStartNodesAuto;
     p.u_split = start_split(prm->n, p.u_first, (uint64_t)kSbTiles * p.tile_nodes, want);
+    const uint64_t st_nodes = (uint64_t)kStartPasses * p.groups;
+    p.start_tiles = (p.u_split - p.u_first + st_nodes - 1) / st_nodes;
+    p.scratch_bytes = p.start_offset + kStartAreaBytes;
+    p.claim_tiles = prm->claim_tiles ? prm->claim_tiles : kClaimTilesAuto;
     *plan = p;
     return PA_OK;
 }
@@ -126,6 +129,7 @@ int pa_params_check(const pa_params *prm)
         return PA_ERR_INVALID;
     if (prm->threads != 0 && prm->threads != 256) return PA_ERR_NOT_SUPPORTED;
     if ((prm->flags & ~PA_FLAG_TEST_WITHHOLD_FIRST_TILE) != 0) return PA_ERR_INVALID;
+    if (prm->claim_tiles > 64 || prm->reserved0 != 0) return PA_ERR_INVALID;
     return PA_OK;
 }
 
@@ -193,8 +197,8 @@ int pa_generate_timed(const pa_params *prm, void *d_edges, uint64_t edges_bytes,
     if ((reinterpret_cast<uintptr_t>(d_edges) & 15u) || (reinterpret_cast<uintptr_t>(d_scratch) & 15u))
         return PA_ERR_INVALID;
     if (edges_bytes < p.edges_bytes || scratch_bytes < p.scratch_bytes) return PA_ERR_CAPACITY;
-    const cudaEvent_t ev[3] = {(cudaEvent_t)events[0], (cudaEvent_t)events[1],
-                               (cudaEvent_t)events[2]};
+    const cudaEvent_t ev[4] = {(cudaEvent_t)events[0], (cudaEvent_t)events[1],
+                               (cudaEvent_t)events[2], (cudaEvent_t)events[3]};
     return launch_generate(prm, p, d_edges, d_scratch, (cudaStream_t)stream, 0, ev);
 }
 

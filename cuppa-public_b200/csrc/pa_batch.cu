@@ -54,6 +54,7 @@ struct BatchArgs {
     unsigned long long t_begin, t_end;      // global tiles of this launch
     unsigned long long *ticket;             // this launch's claim counter
     GenCtl *ctl;                            // shared status and counters
+    uint32_t claim;                         // tiles per claim
 };
 
 template <typename Id, int P>
@@ -78,9 +79,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) batch_kernel(const Batch
         unsigned long long chunk = 0;
         if (L.lane == 0) chunk = atomicAdd(b.ticket, 1ull);
         chunk = __shfl_sync(kFull, chunk, 0);
-        const unsigned long long T0 = b.t_begin + chunk * kClaimTiles;
+        const unsigned long long T0 = b.t_begin + chunk * b.claim;
         if (T0 >= b.t_end) break;
-        for (uint32_t c = 0; c < kClaimTiles && ok; ++c) {
+        for (uint32_t c = 0; c < b.claim && ok; ++c) {
             const unsigned long long T = T0 + c;
             if (T >= b.t_end) break;
             uint32_t i;
@@ -138,7 +139,7 @@ int launch_batch(const BatchArgs &b, cudaStream_t s)
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)kThreads, smem);
     if (e != cudaSuccess) return set_cuda_error(e);
     // no more warps than chunks to claim
-    const unsigned long long chunks = (b.t_end - b.t_begin + kClaimTiles - 1) / kClaimTiles;
+    const unsigned long long chunks = (b.t_end - b.t_begin + b.claim - 1) / b.claim;
     unsigned long long blocks = (unsigned long long)sms * (per_sm > 0 ? per_sm : 1);
     const unsigned long long need = (chunks + kThreads / 32 - 1) / (kThreads / 32);
     if (need < blocks) blocks = need > 0 ? need : 1;
@@ -153,7 +154,7 @@ namespace gen {
 
 int launch_tail(uint32_t id_bytes, uint32_t passes, const GenArgs *d_inst, const LevelTables &tabs,
                 uint32_t count, unsigned long long t_begin, unsigned long long t_end,
-                unsigned long long *d_ticket, GenCtl *ctl, cudaStream_t s)
+                unsigned long long *d_ticket, GenCtl *ctl, uint32_t claim_tiles, cudaStream_t s)
 {
     BatchArgs b;
     b.inst = d_inst;
@@ -163,6 +164,7 @@ int launch_tail(uint32_t id_bytes, uint32_t passes, const GenArgs *d_inst, const
     b.t_end = t_end;
     b.ticket = d_ticket;
     b.ctl = ctl;
+    b.claim = claim_tiles ? claim_tiles : 1u;
     if (t_end <= t_begin) return PA_OK;
     if (id_bytes == 8) {
         switch (passes) {
@@ -232,10 +234,11 @@ int batch_prepare(const pa_params *prms, uint32_t count, BatchJob &J)
     J.count = count;
     J.passes = P;
     J.id_bytes = prms[0].id_bits / 8;
+    J.claim_tiles = prms[0].claim_tiles ? prms[0].claim_tiles : kClaimTilesAuto;
     J.plans.assign(count, GenPlan{});
+    J.max_start_pairs = 0;
     J.flags_off.assign(count, 0);
     J.sb_off.assign(count, 0);
-    J.max_start_pairs = 0;
     std::vector<std::vector<uint64_t>> sb(count), tb(count);
     for (uint32_t i = 0; i < count; ++i) {
         pa_params q = prms[i];
@@ -268,7 +271,7 @@ int batch_prepare(const pa_params *prms, uint32_t count, BatchJob &J)
     }
     J.image_bytes = o - J.image_off;
     J.ticket_off = o;
-    o += 256;
+    o += 128ull * (kStartCounters + 2);   // start counters, tail counter
     for (uint32_t i = 0; i < count; ++i) {
         J.flags_off[i] = o;
         o += al(4 * J.plans[i].n_tiles);
@@ -316,6 +319,8 @@ int batch_bind(BatchJob &J, const pa_params *prms, void *const *d_edges, const u
         a.window_shift = 63;
         a.min_window = 0;
         a.start_end = p.u_split;
+        a.claim_tiles = J.claim_tiles;
+
         std::memcpy(table + i, &a, sizeof(a));
         if (i == 0) J.first = a;
     }
@@ -336,7 +341,9 @@ int batch_enqueue(const BatchJob &J, void *d_scratch, const void *image, cudaStr
         e = cudaMemcpyAsync(scr + J.image_off, image, J.image_bytes, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return set_cuda_error(e);
     const gen::GenArgs *d_inst = reinterpret_cast<const gen::GenArgs *>(scr + J.table_off);
+    // start-kernel counters: kStartCounters lines of 128 bytes; then the tail's
     unsigned long long *tickets = reinterpret_cast<unsigned long long *>(scr + J.ticket_off);
+    unsigned long long *tail_ticket = tickets + 16 * kStartCounters;
     GenCtl *ctl = reinterpret_cast<GenCtl *>(scr);
     int rc = gen::fill_start(J.id_bytes, d_inst, J.count, J.max_start_pairs, s);
     if (rc != PA_OK) return rc;
@@ -353,7 +360,8 @@ int batch_enqueue(const BatchJob &J, void *d_scratch, const void *image, cudaStr
     rc = gen::launch_start(J.id_bytes, sa, 0, s);
     if (rc != PA_OK) return rc;
     return gen::launch_tail(J.id_bytes, J.passes, d_inst, device_tables(J.tail, scr), J.count,
-                            J.tail.lvl[0], J.tail.lvl[J.tail.levels], tickets + 1, ctl, s);
+                            J.tail.lvl[0], J.tail.lvl[J.tail.levels], tail_ticket, ctl,
+                            J.claim_tiles, s);
 }
 
 }  // namespace pa

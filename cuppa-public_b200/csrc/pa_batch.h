@@ -18,13 +18,13 @@ struct BatchLevels {
 };
 
 struct BatchJob {
-    uint32_t count = 0, passes = 0, id_bytes = 0;
+    uint32_t count = 0, passes = 0, id_bytes = 0, claim_tiles = 0;
     std::vector<GenPlan> plans;
     std::vector<uint64_t> flags_off, sb_off;
     BatchLevels start, tail;
-    uint64_t max_start_pairs = 0;
     uint64_t image_off = 0, image_bytes = 0;   // scratch bytes copied from the host image
     uint64_t table_off = 0, ticket_off = 0, scratch_bytes = 0;
+    uint64_t max_start_pairs = 0;       // the largest start region (fill launch size)
     gen::GenArgs first{};                      // instance 0 (the start kernel's count == 1 path)
 };
 

@@ -143,6 +143,13 @@ __device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p)
     return v;
 }
 
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
 // Copy-target reads: strong (L2-coherent) loads.  L1 is not coherent across SMs,
 // and a line holding a finished slot may also hold a neighbour that was still
 // being written when the line was cached, so these reads never use L1.

@@ -42,11 +42,12 @@ struct GenArgs {
     uint64_t *trace;           // progress samples (elapsed ns, nodes complete)
     uint64_t trace_step;       // superblocks between samples
     uint32_t max_sleep_ns;     // back-off cap of dependency waits
-    uint64_t tile_begin;       // first tile of the persistent launch (earlier ones: level launches)
+    uint64_t tile_begin;       // first tile of the persistent launch (earlier ones: start kernel)
     uint64_t water_init;       // superblocks complete when the persistent launch starts
     uint32_t window_shift;     // start gate: a tile at node tb waits for the watermark
     uint64_t min_window;       //   to reach tb - max(min_window, tb >> window_shift)
     uint64_t start_end;        // start kernel: nodes [u_first, start_end) are its work
+    uint32_t claim_tiles;      // tiles per claim-counter atomic
 };
 
 // Record a device-side error once, in the control block and every replica.
@@ -416,8 +417,10 @@ __device__ __forceinline__ void map_unit(const LevelTables &tab, uint32_t count,
     t = __ldg(tab.loc_start + (uint64_t)l * count + inst) + (r - __ldg(ib + inst));
 }
 
-// Warp passes per start tile, the start kernel's unit of work.
-constexpr int kStartPasses = 4;
+// The start kernel's claim counters: warp w of a block claims from counter w,
+// which hands out start tiles w, w + 8, w + 16, ... (one atomic per tile, eight
+// addresses instead of one).
+constexpr uint32_t kStartCounters = kThreads / 32;
 
 // Start kernel (pa_start.cu): start tiles of one graph (count == 1, arguments in
 // `one`) or of `count` graphs in level order (arguments in `inst`).
@@ -428,12 +431,12 @@ struct StartArgs {
     uint32_t count;
     uint32_t write_seeds;          // also write every graph's seed edges
     unsigned long long t_end;      // start tiles of the launch
-    unsigned long long *ticket;    // claim counter (zero at launch)
+    unsigned long long *ticket;    // kStartCounters claim counters, 128 bytes apart (zero)
     GenCtl *ctl;                   // shared status and counters
 };
 
-// Launch the start kernel; `blocks` 0 = one wave.  The target field of every
-// pair of the graphs' start regions must hold all-ones before it runs.
+// Launch the start kernel; `blocks` 0 = one wave.  The claim counters must be
+// zero and every pair of the graphs' start regions all-ones (fill_start).
 int launch_start(uint32_t id_bytes, const StartArgs &b, uint32_t blocks, cudaStream_t s);
 
 // Set every byte of the pairs of nodes [u_first, start_end) of each of `count`
@@ -445,9 +448,8 @@ int fill_start(uint32_t id_bytes, const GenArgs *d_inst, uint32_t count, uint64_
 // graphs; every node of graph i below node u_first + loc_start[l_begin][i] *
 // tile_nodes is complete when it starts.
 int launch_tail(uint32_t id_bytes, uint32_t passes, const GenArgs *d_inst, const LevelTables &tabs,
-                uint32_t count, uint32_t l_begin, unsigned long long t_begin,
-                unsigned long long t_end, unsigned long long *d_ticket, GenCtl *ctl,
-                cudaStream_t s);
+                uint32_t count, unsigned long long t_begin, unsigned long long t_end,
+                unsigned long long *d_ticket, GenCtl *ctl, uint32_t claim_tiles, cudaStream_t s);
 
 }  // namespace gen
 }  // namespace pa

@@ -127,7 +127,7 @@ __device__ __forceinline__ void advance_watermark(const GenArgs &a, uint32_t lan
     }
 }
 
-// Tiles are claimed kClaimTiles at a time: one ticket names a chunk of
+// Tiles are claimed claim_tiles at a time: one ticket names a chunk of
 // consecutive tiles that the warp then takes in order.  The ticket of the next
 // chunk is requested as soon as a chunk is opened, so its round trip is hidden
 // behind the chunk's work.  Chunks are claimed in increasing order by running
@@ -140,10 +140,10 @@ struct Claimer {
 
 __device__ __forceinline__ uint64_t claim_next(Claimer &c, const GenArgs &a, const Lane &L)
 {
-    if (c.idx == kClaimTiles) {
+    if (c.idx == a.claim_tiles) {
         const uint64_t chunk = __shfl_sync(kFull, c.pre, 0);
         if (L.lane == 0) c.pre = atomicAdd(&a.ctl->ticket, 1ull);
-        c.base = a.tile_begin + chunk * kClaimTiles;
+        c.base = a.tile_begin + chunk * a.claim_tiles;
         c.idx = 0;
     }
     return c.base + c.idx++;
@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) gen_kernel(const GenArgs
     // Prologue: the first two tiles and the current watermark.
     Claimer cl;
     cl.base = 0;
-    cl.idx = kClaimTiles;
+    cl.idx = a.claim_tiles;
     cl.pre = 0;
     unsigned long long wt = 0;
     if (L.lane == 0) {
@@ -360,8 +360,9 @@ int launch_passes(const GenArgs &a, uint32_t passes, uint32_t blocks, cudaStream
 int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, void *d_scratch,
                     cudaStream_t stream, uint32_t blocks_override, const cudaEvent_t *events)
 {
-    // optional phase marks: [0] before the first launch, [1] between the start
-    // region and the persistent launch, [2] after the last launch
+    // optional phase marks: [0] before the first launch, [1] before the start
+    // kernel (after the clear and the fill), [2] before the persistent launch,
+    // [3] after the last launch
     auto mark = [&](int i) -> int {
         if (!events || !events[i]) return PA_OK;
         const cudaError_t er = cudaEventRecord(events[i], stream);
@@ -404,6 +405,8 @@ int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, vo
     a.water_init = 0;
 
     a.start_end = plan.u_split;
+    a.claim_tiles = plan.claim_tiles;
+
 
     const uint32_t blocks = blocks_override ? blocks_override : prm->blocks;
     // 32-bit node arithmetic needs every node id, and tile base + tile_nodes,
@@ -411,7 +414,7 @@ int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, vo
     const bool small = prm->n + plan.tile_nodes + 32 < (1ull << 32);
     if (plan.u_split > plan.u_first) {
         // The start region, with slot-granular waits (pa_start.cu): its pairs
-        // start as all-ones, the start kernel writes them and the seed edges.
+        // start as all-ones; the start kernel writes them and the seed edges.
         const uint64_t pair_bytes = 2ull * plan.id_bytes;
         e = cudaMemsetAsync(reinterpret_cast<unsigned char *>(d_edges) + plan.seed_edges * pair_bytes,
                             0xff, (plan.u_split - plan.u_first) * prm->d * pair_bytes, stream);
@@ -421,22 +424,27 @@ int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, vo
         sa.one = a;
         sa.count = 1;
         sa.write_seeds = 1;
-        const uint64_t st_nodes = (uint64_t)kStartPasses * plan.groups;
-        sa.t_end = (plan.u_split - plan.u_first + st_nodes - 1) / st_nodes;
+        sa.t_end = plan.start_tiles;
         sa.ticket = reinterpret_cast<unsigned long long *>(reinterpret_cast<unsigned char *>(d_scratch) +
                                                           plan.start_offset);
         sa.ctl = a.ctl;
+        mrc = mark(1);
+        if (mrc != PA_OK) return mrc;
         const int rc = launch_start(plan.id_bytes, sa, blocks, stream);
         if (rc != PA_OK) return rc;
         if (plan.u_split >= prm->n) {
-            mrc = mark(1);
-            return mrc != PA_OK ? mrc : mark(2);
+            mrc = mark(2);
+            return mrc != PA_OK ? mrc : mark(3);
         }
         // u_split - u_first is a whole number of superblocks
         a.tile_begin = (plan.u_split - plan.u_first) / plan.tile_nodes;
         a.water_init = a.tile_begin / kSbTiles;
     }
-    mrc = mark(1);
+    if (plan.u_split <= plan.u_first) {
+        mrc = mark(1);
+        if (mrc != PA_OK) return mrc;
+    }
+    mrc = mark(2);
     if (mrc != PA_OK) return mrc;
     int rc;
     if (plan.id_bytes == 8)
@@ -444,7 +452,7 @@ int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, vo
                    : launch_passes<int64_t, uint64_t>(a, plan.passes, blocks, stream);
     else
         rc = launch_passes<int32_t, uint32_t>(a, plan.passes, blocks, stream);
-    return rc != PA_OK ? rc : mark(2);
+    return rc != PA_OK ? rc : mark(3);
 }
 
 }  // namespace pa

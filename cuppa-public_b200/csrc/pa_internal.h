@@ -39,9 +39,13 @@ constexpr uint32_t kReps = 16;
 constexpr uint64_t kRepOffset = 256;                        // replicas after GenCtl
 constexpr uint64_t kCtlBytes = kRepOffset + kReps * 128;    // flags start here
 constexpr uint32_t kSbTiles = 64;    // tiles per superblock (watermark granularity)
-constexpr uint32_t kClaimTiles = 4;  // consecutive tiles claimed by one ticket
+constexpr uint32_t kClaimTilesAuto = 4;  // default tiles claimed by one ticket
 constexpr uint32_t kTraceMax = 2048; // progress samples kept per generation
-constexpr uint64_t kStartAreaBytes = 256;  // the start kernel's claim counter
+// the start kernel's claim counters: 8, a 128-byte line each
+constexpr uint64_t kStartAreaBytes = 1024;
+
+// Warp passes per start tile, the start kernel's unit of work.
+constexpr int kStartPasses = 4;
 
 // Resolved launch geometry of one generation.
 struct GenPlan {
@@ -54,8 +58,10 @@ struct GenPlan {
     uint64_t n_sb;          // superblocks of kSbTiles tiles
     uint64_t sb_offset;     // byte offset of the superblock counters in the scratch
     uint64_t trace_offset;  // byte offset of the progress trace in the scratch
-    uint64_t start_offset;  // byte offset of the start kernel's claim counter
+    uint64_t start_offset;  // byte offset of the start kernel's counters
+    uint64_t start_tiles;   // start tiles of the start region
     uint64_t u_split;       // nodes [u_first, u_split) are the start kernel's
+    uint32_t claim_tiles;   // tiles (or start tiles) per claim-counter atomic
     uint64_t seed_edges;
     uint64_t n_edges;
     uint64_t pth;           // direct threshold
@@ -73,8 +79,10 @@ int make_plan(const pa_params *prm, GenPlan *plan);
 // smallest whole number of superblocks covering `want` nodes, capped at n.
 uint64_t start_split(uint64_t n, uint64_t u_first, uint64_t sb_nodes, uint64_t want);
 
-// Default start region: the first 2^24 generated nodes.
-constexpr uint64_t kStartNodesAuto = 1ull << 24;
+// Default start region: every node up to the start kernel's limit of 2^31 (the
+// start kernel, with the memset of its region, outran the persistent kernel at
+// every size measured on B200; the persistent kernel takes nodes beyond).
+constexpr uint64_t kStartNodesAuto = 1ull << 31;
 
 // Launch the generator kernel on `stream` into caller memory; scratch must hold
 // plan.scratch_bytes and is cleared here.

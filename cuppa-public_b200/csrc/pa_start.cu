@@ -1,4 +1,4 @@
-// pa_start.cu -- the start of every graph, with waits on single slots.
+// pa_start.cu -- graphs generated with waits on single slots.
 //
 // Early in a graph most copy reads land on nodes that are still being
 // generated.  The persistent kernel publishes completion per tile, and a tile
@@ -10,8 +10,8 @@
 // 136 tile steps at 8192 nodes, 49 against 365 at 2^18).  With each step a
 // poll round trip, the first few million nodes of a graph cost milliseconds.
 //
-// The start kernel removes the tile from the chain.  Before it runs, every pair
-// of the start region is set to all-ones, which is never a node id.  A lane
+// This kernel takes the tile out of the chain.  Before it runs, every pair of
+// its region is set to all-ones (a memset), which is never a node id.  A lane
 // stores its slot's pair the moment the slot is final -- every lower slot of
 // its node final and its candidate distinct from theirs -- and a copy read of
 // slot (v, k) re-reads that pair's target field until it is not all-ones.  The
@@ -19,14 +19,18 @@
 // so a gpu-scope relaxed load returns either the fill or that value, and no
 // fence, flag or watermark is involved.  Copy sources inside the lane's own
 // warp pass are taken from the source lane by shuffle once it is final, as in
-// the persistent kernel.
+// the persistent kernel.  (Filling inside the kernel instead -- each warp
+// filling the tile it claims, with per-tile opened flags and a watermark for
+// readers -- measured slower on B200 than the memset it saves: 88.7 against
+// 68.0 ms for n = 2^30, d = 4.)
 //
 // Work is claimed one start tile at a time: kStartPasses warp passes of G =
 // 32/d nodes each (lane = node-in-pass * d + slot), resolved together, so a
-// wait in one pass does not hold back the others.  Tiles are claimed in
-// increasing order within each graph: the warp holding the lowest unfinished
-// tile of a graph always progresses and the launch is deadlock-free for any
-// grid.  Several graphs share one launch in level order (pa_gen_core.cuh).
+// wait in one pass does not hold back the others.  Warp w of a block claims
+// from counter w (of kStartCounters), which hands out tiles w, w + 8, ... in
+// increasing order: eight counter lines instead of one, since a single counter
+// saturates at one atomic every few nanoseconds.  Several graphs share one
+// launch in level order (pa_gen_core.cuh).
 //
 // Draws, the slot order and the rejection rule are the persistent kernel's, so
 // the output is bit-identical to it and to the sequential definition
@@ -44,6 +48,21 @@ struct Sentinel {
     static constexpr uint64_t value = sizeof(Id) == 8 ? ~0ull : 0xffffffffull;
 };
 
+// Read slot (v, k) into s: true with its value, or false (s.val = v) while it
+// still holds the fill.
+template <typename Id>
+__device__ __forceinline__ bool read_slot(Slot<uint32_t> &s, const GenArgs &a, const Id *E,
+                                          uint32_t v, uint32_t k)
+{
+    const uint64_t x = ld_slot(slot_addr(E, a, v, k));
+    if (x != Sentinel<Id>::value) {
+        s.val = (uint32_t)x;
+        return true;
+    }
+    s.val = v;
+    return false;
+}
+
 // Where the candidate of a fresh draw comes from (32-bit node arithmetic: the
 // start region ends below 2^31).
 template <typename Id>
@@ -57,11 +76,7 @@ __device__ __forceinline__ void classify_start(Slot<uint32_t> &s, const DrawT<ui
     } else if (dr.v <= a.d) {
         s.val = (uint32_t)seed_slot(dr.v, dr.k, a.d, a.seed_mode);
     } else if (dr.v < pbase) {
-        const uint64_t x = ld_slot(slot_addr(E, a, dr.v, dr.k));
-        if (x != Sentinel<Id>::value) {
-            s.val = (uint32_t)x;
-        } else {
-            s.val = dr.v;
+        if (!read_slot<Id>(s, a, E, dr.v, dr.k)) {
             st = ST_PEND_GLOBAL;
             ++n_pend;
         }
@@ -101,9 +116,7 @@ __device__ __forceinline__ bool resolve_start(Slot<uint32_t> (&s)[kStartPasses],
             const uint32_t u = pbase + L.g;
             const bool active = L.used && u < a.start_end;
             if (active && meta_st(s[j].meta) == ST_PEND_GLOBAL) {
-                const uint64_t x = ld_slot(slot_addr(E, a, s[j].val, meta_k(s[j].meta)));
-                if (x != Sentinel<Id>::value) {
-                    s[j].val = (uint32_t)x;
+                if (read_slot<Id>(s[j], a, E, s[j].val, meta_k(s[j].meta))) {
                     s[j].meta &= ~3u;
                     changed = true;
                 } else {
@@ -215,10 +228,19 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) start_kernel(const Start
 
     uint32_t n_retry = 0, n_wait = 0, n_pend = 0, n_poll = 0;
     bool ok = true;
+    // Counter `warp` hands out tiles warp, warp + 8, ... in increasing order.
+    // Let T* be the lowest unfinished tile.  If it is claimed, its warp is
+    // working on it (a warp holds one tile at a time) and every tile it reads
+    // is lower, hence finished: it progresses.  If not, every tile its counter has handed out is lower,
+    // hence finished, so the warps of that counter are free and the next of
+    // them to claim takes T*.  Any resident block has a warp on every counter,
+    // so this holds for any grid.
+    unsigned long long *my_ticket = b.ticket + 16 * warp;
     while (ok) {
-        unsigned long long T = 0;
-        if (L.lane == 0) T = atomicAdd(b.ticket, 1ull);
-        T = __shfl_sync(kFull, T, 0);
+        unsigned long long c = 0;
+        if (L.lane == 0) c = atomicAdd(my_ticket, 1ull);
+        c = __shfl_sync(kFull, c, 0);
+        const unsigned long long T = c * kStartCounters + warp;
         if (T >= b.t_end) break;
         uint32_t i = 0;
         uint64_t t = T;

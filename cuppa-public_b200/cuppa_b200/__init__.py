@@ -74,6 +74,8 @@ class PaParams(ctypes.Structure):
         ("flags", ctypes.c_uint32),
         ("spin_limit_ns", ctypes.c_uint64),
         ("start_nodes", ctypes.c_uint64),
+        ("claim_tiles", ctypes.c_uint32),
+        ("reserved0", ctypes.c_uint32),
     ]
 
 
@@ -232,13 +234,14 @@ def check(status: int, where: str) -> None:
 def make_params(n: int, d: int, p: float, seed: int = 42, id_bits: int = 32,
                 seed_mode: int = PA_SEED_CLIQUE, blocks: int = 0, threads: int = 0,
                 tile_passes: int = 0, flags: int = 0, spin_limit_ns: int = 0,
-                start_nodes: int = 0) -> PaParams:
+                start_nodes: int = 0, claim_tiles: int = 0) -> PaParams:
     prm = PaParams()
     check(lib().pa_params_init(ctypes.byref(prm)), "pa_params_init")
     prm.n, prm.d, prm.p, prm.seed = n, d, float(p), seed
     prm.id_bits, prm.seed_mode = id_bits, seed_mode
     prm.blocks, prm.threads, prm.tile_passes = blocks, threads, tile_passes
     prm.flags, prm.spin_limit_ns, prm.start_nodes = flags, spin_limit_ns, start_nodes
+    prm.claim_tiles = claim_tiles
     return prm
 
 
@@ -288,13 +291,13 @@ def generate_into(prm: PaParams, edges, scratch, stream=None) -> None:
 
 
 def generate_timed(prm: PaParams, edges, scratch, events, stream=None) -> None:
-    """pa_generate_timed: `events` are three torch.cuda.Event(enable_timing=True)
-    recorded before the first launch, between the start region and the
-    persistent launch, and after the last launch."""
+    """pa_generate_timed: `events` are four torch.cuda.Event(enable_timing=True)
+    recorded before the first launch, before the start kernel, before the
+    persistent launch and after the last launch."""
     for ev in events:
         if not ev.cuda_event:
             ev.record(stream)      # the CUDA event is created on first record
-    arr = (ctypes.c_void_p * 3)(*[ev.cuda_event for ev in events])
+    arr = (ctypes.c_void_p * 4)(*[ev.cuda_event for ev in events])
     rc = lib().pa_generate_timed(ctypes.byref(prm), ctypes.c_void_p(edges.data_ptr()),
                                  edges.numel() * edges.element_size(),
                                  ctypes.c_void_p(scratch.data_ptr()), scratch.numel(),

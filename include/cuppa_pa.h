@@ -77,7 +77,10 @@ typedef struct pa_params {
     uint64_t spin_limit_ns; /* limit of any single device wait; 0 = 2 s                    */
     uint64_t start_nodes;   /* nodes after the seed generated by the start kernel (slot-
                                granular waits); rounded up to whole superblocks of the
-                               persistent launch.  0 = auto, PA_START_NONE = none        */
+                               persistent launch, at most 2^31.  0 = auto (as many as
+                               that allows), PA_START_NONE = none                        */
+    uint32_t claim_tiles;   /* tiles claimed per work-counter atomic (1..64); 0 = auto   */
+    uint32_t reserved0;     /* must be 0                                                  */
 } pa_params;
 
 /* pa_params.start_nodes: no start kernel (the persistent launch does every node). */
@@ -117,11 +120,12 @@ int pa_start_split(const pa_params *prm, uint64_t *u_split);
  * Host-side errors return at once; device-side status is read by pa_generate_finish. */
 int pa_generate(const pa_params *prm, void *d_edges, uint64_t edges_bytes, void *d_scratch,
                 uint64_t scratch_bytes, void *stream);
-/* pa_generate with the phases timed: events[0..2] (cudaEvent_t, any may be
- * NULL) are recorded on `stream` before the first launch, between the start
- * kernel's region and the persistent launch, and after the last launch.  The
- * device side of the per-stage timing table the reference writes
- * (src/PA/cuPPA/cuPPA_1.cu:84-87,217-223). */
+/* pa_generate with the phases timed: events[0..3] (cudaEvent_t, any may be
+ * NULL) are recorded on `stream` before the first launch, before the start
+ * kernel (after the scratch clear and the all-ones fill of its region), before
+ * the persistent launch, and after the last launch.  The device side of the
+ * per-stage timing table the reference writes (src/PA/cuPPA/cuPPA_1.cu:84-87,
+ * 217-223). */
 int pa_generate_timed(const pa_params *prm, void *d_edges, uint64_t edges_bytes, void *d_scratch,
                       uint64_t scratch_bytes, void *stream, void *const *events);
 /* Wait for the stream, then copy the status and counters of the generation that

@@ -94,3 +94,25 @@ def test_generate_rejects_bad_buffers_without_touching_the_device(pa):
     # misaligned
     bad = ctypes.c_void_p(0x10004)
     assert L.pa_generate(ctypes.byref(prm), bad, eb, fake, sb, None) == pa.PA_ERR_INVALID
+
+
+def test_start_split(pa):
+    """Nodes below the split are the start kernel's: all of a graph below 2^31
+    nodes by default, none with PA_START_NONE, otherwise whole superblocks of
+    the persistent launch (64 tiles of 32/d * 2 nodes)."""
+    def split(n, d, sn, bits=64):
+        return pa.start_split(pa.make_params(n, d, 0.5, id_bits=bits, start_nodes=sn))
+    assert split(2 ** 30, 4, 0) == 2 ** 30
+    assert split(2 ** 30, 4, pa.PA_START_NONE) == 5
+    assert split(10 ** 6, 4, 100_000) == 5 + 98 * 1024
+    assert split(2 ** 33, 4, 0) == 5 + 2 ** 31
+    assert split(100, 4, 10 ** 9) == 100
+
+
+def test_claim_tiles_and_reserved_checked(pa):
+    prm = pa.make_params(1000, 4, 0.5, claim_tiles=65)
+    assert pa.lib().pa_params_check(ctypes.byref(prm)) == pa.PA_ERR_INVALID
+    prm = pa.make_params(1000, 4, 0.5, claim_tiles=64)
+    assert pa.lib().pa_params_check(ctypes.byref(prm)) == pa.PA_OK
+    prm.reserved0 = 1
+    assert pa.lib().pa_params_check(ctypes.byref(prm)) == pa.PA_ERR_INVALID

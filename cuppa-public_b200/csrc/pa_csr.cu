@@ -5,21 +5,17 @@
 //
 // Row x is [x's own targets, all < x, ascending] ++ [x's in-neighbours, all > x,
 // ascending], so it comes out sorted when both parts are:
-//   1. in-degrees: one warp-aggregated atomic per pair on its destination; the
-//      value the atomic returns is the pair's rank in the destination's in part,
-//      kept (4 bytes per pair) so that step 4 needs no atomics;
-//   2. rowptr = exclusive scan of out-degree + in-degree: a single-pass scan with
-//      decoupled look-back (tiles take ids in launch order from an atomic counter,
-//      publish their aggregate, then their inclusive prefix);
-//   3. out part: each generated row's d targets ranked in registers and stored;
-//      the seed rows' targets come from the (canonical) seed edges;
-//   4. in part: every pair (u, v) stores u at its rank in v's in part (order
-//      arbitrary across warps) ...
-//   5. ... then every in part is sorted: a warp per part of <= 32 entries (rank
-//      by counting; entries of a part are distinct), a warp bitonic network in
-//      registers for <= 256 entries, a CTA bitonic sort in shared memory for
-//      <= 8192, and the few larger hub parts by a bitmap over the node range
-//      (set, then compact in order).
+//   1. in parts: the pairs, taken as (destination, source) items, are sorted by
+//      destination with a stable LSD radix sort; the pairs are in source order,
+//      so every destination's sources come out ascending, back to back;
+//   2. rowptr[x] = (out entries of rows below x: a closed form) + (items with
+//      destination below x: read off the run boundaries of the sorted items);
+//   3. in part entries: sorted item i with destination v goes to position
+//      outprefix(v + 1) + i;
+//   4. out part: each generated row's d targets ranked in registers and stored;
+//      the seed rows' targets come from the (canonical) seed edges.
+// Items pack (v, u) in 8 bytes, so graphs of 2^32 nodes and more are refused.
+#include <algorithm>
 #include <type_traits>
 #include <vector>
 
@@ -33,7 +29,6 @@ constexpr uint32_t kFull = 0xffffffffu;
 constexpr uint32_t kScanThreads = 256;
 constexpr uint32_t kScanItems = 8;
 constexpr uint32_t kScanTile = kScanThreads * kScanItems;
-constexpr uint32_t kMidMax = 8192;   // largest in part sorted in shared memory
 
 // ---------------------------------------------------------------------------
 // Exclusive scan of int64 with decoupled look-back.  Tile status word:
@@ -190,56 +185,6 @@ __global__ void out_part_kernel(const Id *E, const int64_t *rowptr, Id *col, uin
     }
 }
 
-// ---------------------------------------------------------------------------
-// In-degrees and in-part ranks.
-// ---------------------------------------------------------------------------
-template <typename Id>
-__global__ void in_degree_kernel(const Id *E, uint64_t n_edges, uint64_t n, uint32_t *cnt,
-                                 uint32_t *rank)
-{
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n_edges; base += stride) {
-        const uint64_t e = base + threadIdx.x;
-        unsigned long long v = e < n_edges ? (unsigned long long)E[2 * e + 1] : ~0ull;
-        const bool act = v < n;   // ids are used as addresses: never trust them
-        if (!act) v = ~0ull - lane;
-        const uint32_t peers = __match_any_sync(kFull, v);
-        const uint32_t leader = __ffs(peers) - 1;
-        uint32_t old = 0;
-        if (act && lane == leader) old = atomicAdd(cnt + v, (uint32_t)__popc(peers));
-        old = __shfl_sync(kFull, old, leader);
-        if (act) rank[e] = old + __popc(peers & lanemask_lt());
-    }
-}
-
-// deg[x] = out-degree(x) + in-degree(x); deg[n] = 0 (so rowptr[n] is the total).
-__global__ void deg_fill_kernel(const uint32_t *cnt, const uint32_t *seed_out, uint64_t n,
-                                uint32_t d, int64_t *deg)
-{
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x <= n; x += stride)
-        deg[x] = x == n ? 0 : (int64_t)cnt[x] + (x <= d ? seed_out[x] : d);
-}
-
-// ---------------------------------------------------------------------------
-// In parts: store u at its rank in v's in part (no atomics).
-// ---------------------------------------------------------------------------
-template <typename Id>
-__global__ void in_part_kernel(const Id *E, uint64_t n_edges, uint64_t n, uint32_t d,
-                               const int64_t *rowptr, const uint32_t *rank,
-                               const uint32_t *seed_out, Id *col, uint64_t col_len)
-{
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n_edges; e += stride) {
-        const uint64_t u = (uint64_t)E[2 * e], v = (uint64_t)E[2 * e + 1];
-        if (u >= n || v >= n) continue;   // never trust ids used as addresses
-        const uint64_t outdeg = v <= d ? seed_out[v] : d;
-        const uint64_t pos = (uint64_t)rowptr[v] + outdeg + rank[e];
-        if (pos < (uint64_t)rowptr[v + 1] && pos < col_len) col[pos] = (Id)u;
-    }
-}
-
 // Out-degree of each seed node (its canonical seed edges).
 template <typename Id>
 __global__ void seed_out_kernel(const Id *E, uint64_t seed_edges, uint32_t d, uint32_t *seed_out)
@@ -252,226 +197,218 @@ __global__ void seed_out_kernel(const Id *E, uint64_t seed_edges, uint32_t d, ui
 }
 
 // ---------------------------------------------------------------------------
-// Sorting the in parts.
+// Sorted in parts by a stable LSD radix sort (graphs below 2^32 nodes).
+//
+// Item = (destination v) << 32 | (source u), one per pair.  The pairs are in
+// non-decreasing source order (seed rows, then node d+1, d+2, ...), so a
+// stable sort by v leaves every v's sources ascending: the sorted items are
+// the in parts, in order, back to back.  Item i of the sorted array (key v)
+// goes to col[outprefix(v + 1) + i], where outprefix(x) is the number of out
+// entries of rows below x -- a closed form -- and rowptr[x] = outprefix(x) +
+// (number of items with key < x), read off the run boundaries.  No atomics on
+// the node range, no per-row sorting, no special path for hub rows.
+//
+// A pass sorts 8 key bits: a histogram kernel counts the digits of every tile
+// of 8192 items into a digit-major table, an exclusive scan of the table gives
+// each (digit, tile) its output offset, and the scatter kernel ranks every item
+// within its tile stably -- each warp walks its 1024 items in order, 32 at a
+// time, with __match_any_sync for equal digits and per-warp counters in shared
+// memory, then the warps' counts are prefixed per digit -- and writes it.
 // ---------------------------------------------------------------------------
-template <typename Id>
-__device__ __forceinline__ void in_range(uint64_t x, uint32_t d, const int64_t *rowptr,
-                                         const uint32_t *seed_out, uint64_t &b, uint64_t &len)
-{
-    const uint64_t outdeg = x <= d ? seed_out[x] : d;
-    b = rowptr[x] + outdeg;
-    len = rowptr[x + 1] - b;
-}
+constexpr uint32_t kRadixThreads = 256, kRadixWarps = kRadixThreads / 32;
+constexpr uint32_t kRadixBuckets = 512;   // the widest digit: 9 bits
+constexpr uint32_t kRadixRounds = 32;   // items per lane per tile
+constexpr uint32_t kRadixTile = kRadixThreads * kRadixRounds;
+constexpr unsigned long long kBadKey = 0xffffffffull;   // sorts after every node id
 
-// Small parts (<= 32 entries): one warp each, rank by counting.  Hub parts
-// (> 8192 entries) are queued for the bitmap pass.
-template <typename Id>
-__global__ void sort_small_kernel(uint64_t n, uint32_t d, const int64_t *rowptr,
-                                  const uint32_t *seed_out, Id *col, unsigned long long *big_list,
-                                  unsigned long long *big_count, uint64_t big_cap)
+// Item i of a pass.  The first pass reads the pairs (ids above the node range,
+// never produced by the generator, become kBadKey and raise an error).
+template <typename Id, bool First>
+__device__ __forceinline__ unsigned long long radix_item(const void *src, uint64_t i, uint64_t n,
+                                                         uint32_t *err)
 {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-    const uint64_t w0 = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    for (uint64_t x0 = w0 * 32; x0 < n; x0 += warps * 32) {
-        // each lane classifies one row; then the warp sorts the small ones
-        const uint64_t x = x0 + lane;
-        uint64_t b = 0, len = 0;
-        if (x < n) in_range<Id>(x, d, rowptr, seed_out, b, len);
-        if (len > kMidMax) {
-            const unsigned long long slot = atomicAdd(big_count, 1ull);
-            if (slot < big_cap) big_list[slot] = x;
+    if constexpr (First) {
+        const Id *E = reinterpret_cast<const Id *>(src);
+        const uint64_t u = (uint64_t)E[2 * i], v = (uint64_t)E[2 * i + 1];
+        if (u >= n || v >= n) {
+            atomicCAS(err, 0u, (uint32_t)PA_ERR_INVALID);
+            return (kBadKey << 32) | 0xffffffffull;
         }
-        uint32_t todo = __ballot_sync(kFull, len > 1 && len <= 32);
-        while (todo) {
-            const uint32_t src = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const uint64_t sb = __shfl_sync(kFull, b, src);
-            const uint32_t sl = (uint32_t)__shfl_sync(kFull, len, src);
-            Id val = lane < sl ? col[sb + lane] : (Id)0;
-            uint32_t rank = 0;
-            for (uint32_t j = 0; j < sl; ++j) {
-                const Id o = __shfl_sync(kFull, val, j);
-                rank += (o < val) ? 1u : 0u;
-            }
-            __syncwarp();
-            if (lane < sl) col[sb + rank] = val;
-            __syncwarp();
-        }
+        return (v << 32) | u;
+    } else {
+        return reinterpret_cast<const unsigned long long *>(src)[i];
     }
 }
 
-// Bitonic sort of N = 32*EL values held by a warp, element i = j*32 + lane in
-// v[j]; ascending.  Partners at distance s < 32 are in other lanes (shuffle),
-// at s >= 32 in the same lane.
-template <typename Id, int EL>
-__device__ __forceinline__ void warp_bitonic(Id (&v)[EL], uint32_t lane)
+template <typename Id, bool First, uint32_t DB>
+__global__ void __launch_bounds__(kRadixThreads) radix_hist_kernel(const void *src, uint64_t n_items,
+                                                                   uint32_t shift, uint64_t n,
+                                                                   int64_t *table, uint64_t n_tiles,
+                                                                   uint32_t *err)
 {
-    constexpr uint32_t N = 32u * EL;
-#pragma unroll
-    for (uint32_t k = 2; k <= N; k <<= 1) {
-#pragma unroll
-        for (uint32_t s = k >> 1; s > 0; s >>= 1) {
-            if (s >= 32) {
-                const uint32_t js = s >> 5;
-#pragma unroll
-                for (uint32_t j = 0; j < (uint32_t)EL; ++j) {
-                    const uint32_t jp = j ^ js;
-                    if (jp > j) {
-                        const uint32_t i = j * 32 + lane;
-                        const bool up = (i & k) == 0;
-                        const Id a = v[j], b = v[jp];
-                        if ((a > b) == up) {
-                            v[j] = b;
-                            v[jp] = a;
-                        }
-                    }
-                }
-            } else {
-#pragma unroll
-                for (uint32_t j = 0; j < (uint32_t)EL; ++j) {
-                    const uint32_t i = j * 32 + lane;
-                    const Id o = __shfl_xor_sync(kFull, v[j], s);
-                    const bool up = (i & k) == 0;
-                    const bool lower = (i & s) == 0;   // i < partner
-                    v[j] = (lower == up) ? (v[j] < o ? v[j] : o) : (v[j] > o ? v[j] : o);
-                }
-            }
+    constexpr uint32_t NB = 1u << DB, MASK = NB - 1;
+    __shared__ uint32_t cnt[NB];
+    for (uint32_t b = threadIdx.x; b < NB; b += kRadixThreads) cnt[b] = 0;
+    __syncthreads();
+    const uint64_t t = blockIdx.x;
+    const uint64_t base = t * kRadixTile;
+    for (uint32_t r = 0; r < kRadixRounds; ++r) {
+        const uint64_t i = base + (uint64_t)r * kRadixThreads + threadIdx.x;
+        if (i < n_items) {
+            const unsigned long long it = radix_item<Id, First>(src, i, n, err);
+            atomicAdd(&cnt[(uint32_t)(it >> (32 + shift)) & MASK], 1u);
         }
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < NB; b += kRadixThreads) table[(uint64_t)b * n_tiles + t] = cnt[b];
+}
+
+// Dynamic shared memory of the scatter kernel: the tile's items in digit order,
+// then the per-warp counts, ranks and bases.
+template <uint32_t NB>
+struct RadixSmem {
+    unsigned long long stage[kRadixTile];
+    unsigned long long goff[NB];                  // this tile's global offset per digit
+    uint32_t wcnt[kRadixWarps][NB];               // per-warp digit counts, then bases
+    uint32_t lstart[NB];                          // digit start within the tile
+    uint16_t lrank[kRadixTile];                   // rank within the warp's items of its digit
+};
+
+template <typename Id, bool First, uint32_t DB>
+__global__ void __launch_bounds__(kRadixThreads) radix_scatter_kernel(const void *src,
+                                                                      unsigned long long *dst,
+                                                                      uint64_t n_items, uint32_t shift,
+                                                                      uint64_t n, const int64_t *offs,
+                                                                      uint64_t n_tiles, uint32_t *err)
+{
+    constexpr uint32_t NB = 1u << DB, MASK = NB - 1, PER = NB / kRadixThreads;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    RadixSmem<NB> &S = *reinterpret_cast<RadixSmem<NB> *>(smem_raw);
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t lt = lanemask_lt();
+    for (uint32_t w = 0; w < kRadixWarps; ++w)
+        for (uint32_t b = threadIdx.x; b < NB; b += kRadixThreads) S.wcnt[w][b] = 0;
+    __syncthreads();
+    const uint64_t t = blockIdx.x;
+    const uint64_t tb = t * kRadixTile;
+    const uint32_t tcount = (uint32_t)min((uint64_t)kRadixTile, n_items - tb);
+    const uint32_t wo = warp * (kRadixRounds * 32);
+    // 1. stable ranks within the warp's items (in order, 32 per round)
+    for (uint32_t r = 0; r < kRadixRounds; ++r) {
+        const uint32_t k = wo + r * 32 + lane;
+        const bool valid = k < tcount;
+        uint32_t dg = NB + lane;   // unique for lanes past the end
+        if (valid) dg = (uint32_t)(radix_item<Id, First>(src, tb + k, n, err) >> (32 + shift)) & MASK;
+        const uint32_t peers = __match_any_sync(kFull, dg);
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t old = 0;
+        if (valid && lane == leader) {
+            old = S.wcnt[warp][dg];
+            S.wcnt[warp][dg] = old + __popc(peers);
+        }
+        old = __shfl_sync(kFull, old, leader);
+        if (valid) S.lrank[k] = (uint16_t)(old + __popc(peers & lt));
+    }
+    __syncthreads();
+    // 2. per digit (thread j owns digits j*PER .. j*PER+PER-1): warp bases in
+    // warp order, the digit's total, then the digits' starts within the tile
+    uint32_t tot[PER];
+    uint32_t mine = 0;
+#pragma unroll
+    for (uint32_t q = 0; q < PER; ++q) {
+        const uint32_t dg = threadIdx.x * PER + q;
+        uint32_t acc = 0;
+        for (uint32_t w = 0; w < kRadixWarps; ++w) {
+            const uint32_t c = S.wcnt[w][dg];
+            S.wcnt[w][dg] = acc;
+            acc += c;
+        }
+        tot[q] = acc;
+        mine += acc;
+        S.goff[dg] = (unsigned long long)offs[(uint64_t)dg * n_tiles + t];
+    }
+    uint32_t x = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    __shared__ uint32_t s_wsum[kRadixWarps];
+    if (lane == 31) s_wsum[warp] = x;
+    __syncthreads();
+    uint32_t run = x - mine;
+    for (uint32_t w = 0; w < warp; ++w) run += s_wsum[w];
+#pragma unroll
+    for (uint32_t q = 0; q < PER; ++q) {
+        S.lstart[threadIdx.x * PER + q] = run;
+        run += tot[q];
+    }
+    __syncthreads();
+    // 3. the tile's items into shared memory in digit order (read again, from L2)
+    for (uint32_t r = 0; r < kRadixRounds; ++r) {
+        const uint32_t k = wo + r * 32 + lane;
+        if (k < tcount) {
+            const unsigned long long it = radix_item<Id, First>(src, tb + k, n, err);
+            const uint32_t dg = (uint32_t)(it >> (32 + shift)) & MASK;
+            S.stage[S.lstart[dg] + S.wcnt[warp][dg] + S.lrank[k]] = it;
+        }
+    }
+    __syncthreads();
+    // 4. out in digit runs: consecutive threads write consecutive addresses
+    for (uint32_t k = threadIdx.x; k < tcount; k += kRadixThreads) {
+        const unsigned long long it = S.stage[k];
+        const uint32_t dg = (uint32_t)(it >> (32 + shift)) & MASK;
+        dst[S.goff[dg] + (k - S.lstart[dg])] = it;
     }
 }
 
-template <typename Id, int EL>
-__device__ __forceinline__ void warp_sort_part(Id *col, uint64_t b, uint32_t len, uint32_t lane)
+// Out entries of rows below x: seed rows from their prefix table, then d per row.
+__device__ __forceinline__ uint64_t outprefix(uint64_t x, uint32_t d, uint64_t seed_edges,
+                                              const int64_t *seed_pre)
 {
-    const Id pad = (Id)(~(typename std::make_unsigned<Id>::type)0 >> 1);
-    Id v[EL];
-#pragma unroll
-    for (int j = 0; j < EL; ++j) {
-        const uint32_t i = j * 32 + lane;
-        v[j] = i < len ? col[b + i] : pad;
-    }
-    warp_bitonic<Id, EL>(v, lane);
-#pragma unroll
-    for (int j = 0; j < EL; ++j) {
-        const uint32_t i = j * 32 + lane;
-        if (i < len) col[b + i] = v[j];
-    }
+    return x <= (uint64_t)d + 1 ? (uint64_t)seed_pre[x] : seed_edges + (x - d - 1) * d;
 }
 
-// Parts of 33..256 entries: one warp each, the register bitonic network.
-template <typename Id>
-__global__ void sort_warp_kernel(uint64_t n, uint32_t d, const int64_t *rowptr,
-                                 const uint32_t *seed_out, Id *col)
+// seed_pre[x] = out entries of seed rows below x, x = 0..d+1.
+__global__ void seed_prefix_kernel(const uint32_t *seed_out, uint32_t d, int64_t *seed_pre)
 {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-    const uint64_t w0 = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    for (uint64_t x0 = w0 * 32; x0 < n; x0 += warps * 32) {
-        const uint64_t x = x0 + lane;
-        uint64_t b = 0, len = 0;
-        if (x < n) in_range<Id>(x, d, rowptr, seed_out, b, len);
-        uint32_t todo = __ballot_sync(kFull, len > 32 && len <= 256);
-        while (todo) {
-            const uint32_t src = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const uint64_t sb = __shfl_sync(kFull, b, src);
-            const uint32_t sl = (uint32_t)__shfl_sync(kFull, len, src);
-            if (sl <= 64) warp_sort_part<Id, 2>(col, sb, sl, lane);
-            else if (sl <= 128) warp_sort_part<Id, 4>(col, sb, sl, lane);
-            else warp_sort_part<Id, 8>(col, sb, sl, lane);
-        }
-    }
-}
-
-// Parts of 257..8192 entries: a CTA tests 512 rows at a time, queues those in
-// shared memory and bitonic-sorts each in shared memory.
-template <typename Id>
-__global__ void __launch_bounds__(512) sort_mid_kernel(uint64_t n, uint32_t d, const int64_t *rowptr,
-                                                       const uint32_t *seed_out, Id *col)
-{
-    extern __shared__ __align__(16) unsigned char smem[];
-    Id *buf = reinterpret_cast<Id *>(smem);
-    __shared__ unsigned long long s_rows[512];
-    __shared__ unsigned int s_cnt;
-    for (uint64_t r0 = (uint64_t)blockIdx.x * blockDim.x; r0 < n; r0 += (uint64_t)gridDim.x * blockDim.x) {
-        if (threadIdx.x == 0) s_cnt = 0;
-        __syncthreads();
-        const uint64_t x = r0 + threadIdx.x;
-        if (x < n) {
-            uint64_t b, len;
-            in_range<Id>(x, d, rowptr, seed_out, b, len);
-            if (len > 256 && len <= kMidMax) s_rows[atomicAdd(&s_cnt, 1u)] = x;
-        }
-        __syncthreads();
-        const uint32_t cnt = s_cnt;
-        for (uint32_t m = 0; m < cnt; ++m) {
-            uint64_t b, len;
-            in_range<Id>(s_rows[m], d, rowptr, seed_out, b, len);
-            uint32_t N = 512;
-            while (N < len) N <<= 1;
-            for (uint32_t i = threadIdx.x; i < N; i += blockDim.x)
-                buf[i] = i < len ? col[b + i] : (Id)(~(typename std::make_unsigned<Id>::type)0 >> 1);
-            __syncthreads();
-            for (uint32_t k = 2; k <= N; k <<= 1) {
-                for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-                    for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
-                        const uint32_t ixj = i ^ j;
-                        if (ixj > i) {
-                            const bool up = (i & k) == 0;
-                            const Id a = buf[i], c = buf[ixj];
-                            if ((a > c) == up) {
-                                buf[i] = c;
-                                buf[ixj] = a;
-                            }
-                        }
-                    }
-                    __syncthreads();
-                }
-            }
-            for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) col[b + i] = buf[i];
-            __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t acc = 0;
+        for (uint32_t x = 0; x <= d + 1; ++x) {
+            seed_pre[x] = acc;
+            if (x <= d) acc += seed_out[x];
         }
     }
 }
 
-// Large parts: bitmap over node ids (x, n): set one bit per entry, then write the
-// set bits in order.  The entries of an in part are distinct and all > x.
-template <typename Id>
-__global__ void bitmap_set_kernel(const Id *col, uint64_t b, uint64_t len, uint64_t lo,
-                                  uint64_t n, uint32_t *bits)
+// rowptr[x] = outprefix(x) + #items with key < x, from the sorted keys: item i
+// writes every x in (key(i-1), key(i)]; i = n_items closes the range up to n.
+__global__ void rowptr_kernel(const unsigned long long *items, uint64_t n_items, uint64_t n,
+                              uint32_t d, uint64_t seed_edges, const int64_t *seed_pre,
+                              int64_t *rowptr)
 {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += stride) {
-        const uint64_t x = (uint64_t)col[b + i];
-        if (x < lo || x >= n) continue;
-        const uint64_t v = x - lo;
-        atomicOr(bits + (v >> 5), 1u << (v & 31));
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n_items; i += stride) {
+        const uint64_t hi = i < n_items ? min((uint64_t)(items[i] >> 32), n) : n;
+        const uint64_t lo = i > 0 ? min((uint64_t)(items[i - 1] >> 32), n) + 1 : 0;
+        for (uint64_t x = lo; x <= hi && x <= n; ++x)
+            rowptr[x] = (int64_t)(outprefix(x, d, seed_edges, seed_pre) + i);
     }
 }
 
-// Per 32-bit word: population count (pass 1) then ordered write (pass 2) using
-// an exclusive scan of the word counts computed by scan_kernel on int64 counts.
-__global__ void bitmap_count_kernel(const uint32_t *bits, uint64_t words, int64_t *counts)
-{
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += stride)
-        counts[w] = __popc(bits[w]);
-}
-
+// In parts: sorted item i (key v, value u) to col[outprefix(v + 1) + i].
 template <typename Id>
-__global__ void bitmap_write_kernel(const uint32_t *bits, uint64_t words, const int64_t *offs,
-                                    uint64_t lo, Id *col, uint64_t b, uint64_t len)
+__global__ void in_sorted_kernel(const unsigned long long *items, uint64_t n_items, uint64_t n,
+                                 uint32_t d, uint64_t seed_edges, const int64_t *seed_pre, Id *col,
+                                 uint64_t col_len)
 {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += stride) {
-        uint32_t m = bits[w];
-        uint64_t o = (uint64_t)offs[w];
-        while (m && o < len) {
-            const uint32_t bit = __ffs(m) - 1;
-            m &= m - 1;
-            col[b + o++] = (Id)(lo + w * 32 + bit);
-        }
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_items; i += stride) {
+        const unsigned long long it = items[i];
+        const uint64_t v = it >> 32;
+        if (v >= n) continue;
+        const uint64_t pos = outprefix(v + 1, d, seed_edges, seed_pre) + i;
+        if (pos < col_len) col[pos] = (Id)(it & 0xffffffffull);
     }
 }
 
@@ -486,29 +423,29 @@ int grid_for(uint64_t items, uint32_t threads, uint32_t per_sm = 8)
 }
 
 struct CsrLayout {
-    uint64_t deg_off, status_off, ctr_off, err_off, seed_out_off, cursor_off, rank_off, lists_off,
-        bits_off, counts_off, total;
-    uint64_t n_tiles, big_cap, bit_words;
+    uint64_t status_off, ctr_off, err_off, seed_out_off, seed_pre_off, items_off, table_off, total;
+    uint64_t n_tiles;   // scan tiles the status region holds
+    uint64_t r_tiles;   // radix tiles
 };
+
+// Graphs below 2^32 nodes: items pack (v, u) in 8 bytes.
+bool csr_supported(uint64_t n) { return n < (1ull << 32); }
 
 CsrLayout csr_layout(uint64_t n, uint32_t d, uint64_t n_edges)
 {
     auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
     CsrLayout L{};
-    L.n_tiles = (n + 1 + kScanTile - 1) / kScanTile;
-    L.big_cap = (n * d) / 4096 + 16;   // hub parts above 8192 entries: at most 2E / 8192
-    L.bit_words = (n + 31) / 32 + 1;
+    L.r_tiles = (n_edges + kRadixTile - 1) / kRadixTile;
+    const uint64_t scan_len = std::max<uint64_t>(kRadixBuckets * L.r_tiles, n + 1);
+    L.n_tiles = (scan_len + kScanTile - 1) / kScanTile;
     uint64_t o = 0;
-    L.deg_off = o;        o += al(8 * (n + 1));
-    L.status_off = o;     o += al(8 * L.n_tiles);
-    L.ctr_off = o;        o += 256;                       // scan tile counter + list counters
-    L.err_off = o;        o += 256;
-    L.seed_out_off = o;   o += al(4 * (d + 1));
-    L.cursor_off = o;     o += al(4 * n);                  // in-degree counts
-    L.rank_off = o;       o += al(4 * n_edges);            // rank of each pair in its in part
-    L.lists_off = o;      o += al(8 * L.big_cap);
-    L.bits_off = o;       o += al(4 * L.bit_words);
-    L.counts_off = o;     o += al(8 * (L.bit_words + 1));
+    L.items_off = o;    o += al(8 * std::max<uint64_t>(n_edges, 1));
+    L.table_off = o;    o += al(8 * kRadixBuckets * std::max<uint64_t>(L.r_tiles, 1));
+    L.status_off = o;   o += al(8 * L.n_tiles);
+    L.ctr_off = o;      o += 256;
+    L.err_off = o;      o += 256;
+    L.seed_out_off = o; o += al(4 * (d + 1));
+    L.seed_pre_off = o; o += al(8 * (d + 2));
     L.total = o;
     return L;
 }
@@ -531,87 +468,81 @@ int run_scan(const int64_t *in, int64_t *out, uint64_t len, unsigned char *scrat
     return e == cudaSuccess ? PA_OK : set_cuda_error(e);
 }
 
+// One stable pass over DB key bits from `shift` (histogram, scan, scatter).
+template <typename Id, uint32_t DB>
+int radix_pass(bool first, const void *src, unsigned long long *dst, uint64_t m, uint32_t shift,
+               uint64_t n, int64_t *table, unsigned char *scratch, const CsrLayout &L, uint32_t *err,
+               cudaStream_t s)
+{
+    constexpr uint32_t NB = 1u << DB;
+    const unsigned tiles = (unsigned)L.r_tiles;
+    const size_t smem = sizeof(RadixSmem<NB>);
+    cudaError_t e = cudaFuncSetAttribute(radix_scatter_kernel<Id, true, DB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(radix_scatter_kernel<Id, false, DB>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    if (first)
+        radix_hist_kernel<Id, true, DB><<<tiles, kRadixThreads, 0, s>>>(src, m, shift, n, table,
+                                                                        L.r_tiles, err);
+    else
+        radix_hist_kernel<Id, false, DB><<<tiles, kRadixThreads, 0, s>>>(src, m, shift, n, table,
+                                                                         L.r_tiles, err);
+    const int rc = run_scan(table, table, (uint64_t)NB * L.r_tiles, scratch, L, s);
+    if (rc != PA_OK) return rc;
+    if (first)
+        radix_scatter_kernel<Id, true, DB><<<tiles, kRadixThreads, smem, s>>>(src, dst, m, shift, n,
+                                                                              table, L.r_tiles, err);
+    else
+        radix_scatter_kernel<Id, false, DB><<<tiles, kRadixThreads, smem, s>>>(src, dst, m, shift, n,
+                                                                               table, L.r_tiles, err);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? PA_OK : set_cuda_error(e);
+}
+
+// Sort, rowptr, in parts, out parts; one synchronisation at the end for the
+// error word.
 template <typename Id>
 int build_csr(const pa_params *prm, const GenPlan &p, const Id *E, int64_t *rowptr, Id *col,
-              unsigned char *scratch, const CsrLayout &L, cudaStream_t s)
+                     unsigned char *scratch, const CsrLayout &L, cudaStream_t s)
 {
-    const uint64_t n = prm->n;
+    const uint64_t n = prm->n, m = p.n_edges;
     const uint32_t d = prm->d;
-    int64_t *deg = (int64_t *)(scratch + L.deg_off);
     uint32_t *seed_out = (uint32_t *)(scratch + L.seed_out_off);
-    uint32_t *cursor = (uint32_t *)(scratch + L.cursor_off);
-    unsigned long long *lists = (unsigned long long *)(scratch + L.lists_off);
-    unsigned long long *ctrs = (unsigned long long *)(scratch + L.ctr_off);
+    int64_t *seed_pre = (int64_t *)(scratch + L.seed_pre_off);
     uint32_t *err = (uint32_t *)(scratch + L.err_off);
-
-    uint32_t *rank = (uint32_t *)(scratch + L.rank_off);
+    int64_t *table = (int64_t *)(scratch + L.table_off);
+    unsigned long long *A = (unsigned long long *)(scratch + L.items_off);
+    // the column buffer (>= 8 bytes per pair) holds the other ping-pong array
+    // while sorting; the last pass always lands in A
+    unsigned long long *B = reinterpret_cast<unsigned long long *>(col);
     cudaError_t e = cudaMemsetAsync(err, 0, 4, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(cursor, 0, 4 * n, s);
     if (e != cudaSuccess) return set_cuda_error(e);
-
     seed_out_kernel<Id><<<1, 64, 0, s>>>(E, p.seed_edges, d, seed_out);
-    if (p.n_edges)
-        in_degree_kernel<Id><<<grid_for(p.n_edges, 256), 256, 0, s>>>(E, p.n_edges, n, cursor, rank);
-    deg_fill_kernel<<<grid_for(n + 1, 256), 256, 0, s>>>(cursor, seed_out, n, d, deg);
-    int rc = run_scan(deg, rowptr, n + 1, scratch, L, s);   // deg[n] = 0: rowptr[n] = total
-    if (rc != PA_OK) return rc;
-
-    const uint64_t col_len = 2 * p.n_edges;
+    seed_prefix_kernel<<<1, 32, 0, s>>>(seed_out, d, seed_pre);
+    uint32_t bits = 1;
+    while (bits < 32 && (n >> bits) != 0) ++bits;   // keys < n need bits(n) bits; kBadKey sorts last
+    // 9-bit digits when three passes cover the key (n < 2^27), else 8-bit ones
+    const uint32_t db = bits <= 27 ? 9u : 8u;
+    const uint32_t passes = (bits + db - 1) / db;
+    int rc = PA_OK;
+    for (uint32_t q = 0; q < passes && m > 0; ++q) {
+        const uint32_t shift = db * q;
+        unsigned long long *dst = ((passes - 1 - q) % 2 == 0) ? A : B;
+        const void *src = q == 0 ? (const void *)E : (const void *)(((passes - q) % 2 == 0) ? A : B);
+        rc = db == 9 ? radix_pass<Id, 9>(q == 0, src, dst, m, shift, n, table, scratch, L, err, s)
+                     : radix_pass<Id, 8>(q == 0, src, dst, m, shift, n, table, scratch, L, err, s);
+        if (rc != PA_OK) return rc;
+    }
+    rowptr_kernel<<<grid_for(m + 1, 256), 256, 0, s>>>(A, m, n, d, p.seed_edges, seed_pre, rowptr);
+    const uint64_t col_len = 2 * m;
+    in_sorted_kernel<Id><<<grid_for(m, 256), 256, 0, s>>>(A, m, n, d, p.seed_edges, seed_pre, col,
+                                                          col_len);
     out_part_kernel<Id><<<grid_for(n * d, 256), 256, 0, s>>>(E, rowptr, col, n, d, p.seed_edges,
                                                              col_len);
-    in_part_kernel<Id><<<grid_for(p.n_edges, 256), 256, 0, s>>>(E, p.n_edges, n, d, rowptr, rank,
-                                                                seed_out, col, col_len);
-    // list counters live after the scan tile counter
-    e = cudaMemsetAsync(ctrs + 1, 0, 16, s);
-    if (e != cudaSuccess) return set_cuda_error(e);
-    unsigned long long *big_list = lists;
-    sort_small_kernel<Id><<<grid_for(n, 256), 256, 0, s>>>(n, d, rowptr, seed_out, col, big_list,
-                                                           ctrs + 2, L.big_cap);
-    sort_warp_kernel<Id><<<grid_for(n, 256), 256, 0, s>>>(n, d, rowptr, seed_out, col);
-    const size_t smem = kMidMax * sizeof(Id);
-    e = cudaFuncSetAttribute(sort_mid_kernel<Id>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-    if (e != cudaSuccess) return set_cuda_error(e);
-    sort_mid_kernel<Id><<<grid_for(n, 512, 4), 512, smem, s>>>(n, d, rowptr, seed_out, col);
     e = cudaGetLastError();
     if (e != cudaSuccess) return set_cuda_error(e);
-
-    // Large parts: few; the host reads their list and handles them one by one.
-    unsigned long long counts[2] = {0, 0};
-    e = cudaMemcpyAsync(counts, ctrs + 1, 16, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return set_cuda_error(e);
-    if (counts[1] > L.big_cap) return PA_ERR_CAPACITY;
-    if (counts[1]) {
-        std::vector<unsigned long long> big(counts[1]);
-        big_list = lists;
-        e = cudaMemcpyAsync(big.data(), big_list, 8 * counts[1], cudaMemcpyDeviceToHost, s);
-        std::vector<int64_t> rp(2);
-        std::vector<uint32_t> so(d + 1);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(so.data(), seed_out, 4 * (d + 1), cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) return set_cuda_error(e);
-        uint32_t *bits = (uint32_t *)(scratch + L.bits_off);
-        int64_t *wcounts = (int64_t *)(scratch + L.counts_off);
-        for (unsigned long long x : big) {
-            e = cudaMemcpyAsync(rp.data(), rowptr + x, 16, cudaMemcpyDeviceToHost, s);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-            if (e != cudaSuccess) return set_cuda_error(e);
-            const uint64_t outdeg = x <= d ? so[x] : d;
-            const uint64_t b = rp[0] + outdeg, len = rp[1] - b;
-            const uint64_t lo = x + 1, words = (n - lo + 31) / 32;
-            e = cudaMemsetAsync(bits, 0, 4 * words, s);
-            if (e != cudaSuccess) return set_cuda_error(e);
-            bitmap_set_kernel<Id><<<grid_for(len, 256), 256, 0, s>>>(col, b, len, lo, n, bits);
-            bitmap_count_kernel<<<grid_for(words, 256), 256, 0, s>>>(bits, words, wcounts);
-            rc = run_scan(wcounts, wcounts, words, scratch, L, s);
-            if (rc != PA_OK) return rc;
-            bitmap_write_kernel<Id><<<grid_for(words, 256), 256, 0, s>>>(bits, words, wcounts, lo,
-                                                                         col, b, len);
-            e = cudaGetLastError();
-            if (e != cudaSuccess) return set_cuda_error(e);
-        }
-    }
     uint32_t herr = 0;
     e = cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -633,6 +564,7 @@ int pa_csr_bytes(const pa_params *prm, uint64_t *rowptr_bytes, uint64_t *col_byt
     const int rc = make_plan(prm, &p);
     if (rc != PA_OK) return rc;
     if (!rowptr_bytes || !col_bytes || !scratch_bytes) return PA_ERR_INVALID;
+    if (!csr_supported(prm->n)) return PA_ERR_NOT_SUPPORTED;
     *rowptr_bytes = 8 * (prm->n + 1);
     *col_bytes = 2 * p.n_edges * p.id_bytes;
     *scratch_bytes = csr_layout(prm->n, prm->d, p.n_edges).total;
@@ -646,6 +578,9 @@ int pa_build_csr(const pa_params *prm, const void *d_edges, int64_t *d_rowptr, v
     const int rc = make_plan(prm, &p);
     if (rc != PA_OK) return rc;
     if (!d_edges || !d_rowptr || !d_col || !d_scratch) return PA_ERR_INVALID;
+    if (!csr_supported(prm->n)) return PA_ERR_NOT_SUPPORTED;
+    if ((reinterpret_cast<uintptr_t>(d_col) & 15u) || (reinterpret_cast<uintptr_t>(d_scratch) & 15u))
+        return PA_ERR_INVALID;
     const CsrLayout L = csr_layout(prm->n, prm->d, p.n_edges);
     if (scratch_bytes < L.total) return PA_ERR_CAPACITY;
     if (p.id_bytes == 8)

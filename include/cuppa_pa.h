@@ -172,9 +172,10 @@ int pa_degrees(const pa_params *prm, const void *d_edges, int64_t *d_deg, void *
  * Sizes of the three buffers: */
 int pa_csr_bytes(const pa_params *prm, uint64_t *rowptr_bytes, uint64_t *col_bytes,
                  uint64_t *scratch_bytes);
-/* Builds the CSR on `stream` and waits for it (it reads back the list of hub
- * rows, those with more than 8192 in-neighbours, and sorts each of them with a
- * bitmap pass over the node range). */
+/* Builds the CSR on `stream` and waits for it (for its error word).  The in
+ * parts come from a stable radix sort of the pairs by destination; the column
+ * buffer doubles as sort space during the call.  d_col and d_scratch must be
+ * 16-byte aligned.  Graphs of 2^32 nodes or more: PA_ERR_NOT_SUPPORTED. */
 int pa_build_csr(const pa_params *prm, const void *d_edges, int64_t *d_rowptr, void *d_col,
                  void *d_scratch, uint64_t scratch_bytes, void *stream);
 

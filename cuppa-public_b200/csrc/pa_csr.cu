@@ -501,11 +501,11 @@ int radix_pass(bool first, const void *src, unsigned long long *dst, uint64_t m,
     return e == cudaSuccess ? PA_OK : set_cuda_error(e);
 }
 
-// Sort, rowptr, in parts, out parts; one synchronisation at the end for the
-// error word.
+// Sort, rowptr, in parts, out parts, queued on s; the device error word is at
+// scratch + err_off (PA_OK, or PA_ERR_INVALID / PA_ERR_SPIN_TIMEOUT).
 template <typename Id>
-int build_csr(const pa_params *prm, const GenPlan &p, const Id *E, int64_t *rowptr, Id *col,
-                     unsigned char *scratch, const CsrLayout &L, cudaStream_t s)
+int csr_enqueue_t(const pa_params *prm, const GenPlan &p, const Id *E, int64_t *rowptr, Id *col,
+                  unsigned char *scratch, const CsrLayout &L, cudaStream_t s)
 {
     const uint64_t n = prm->n, m = p.n_edges;
     const uint32_t d = prm->d;
@@ -542,15 +542,31 @@ int build_csr(const pa_params *prm, const GenPlan &p, const Id *E, int64_t *rowp
     out_part_kernel<Id><<<grid_for(n * d, 256), 256, 0, s>>>(E, rowptr, col, n, d, p.seed_edges,
                                                              col_len);
     e = cudaGetLastError();
-    if (e != cudaSuccess) return set_cuda_error(e);
-    uint32_t herr = 0;
-    e = cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return set_cuda_error(e);
-    return (int)herr;
+    return e == cudaSuccess ? PA_OK : set_cuda_error(e);
 }
 
 }  // namespace
+
+int csr_enqueue(const pa_params *prm, const void *d_edges, int64_t *d_rowptr, void *d_col,
+                void *d_scratch, uint64_t scratch_bytes, cudaStream_t s, uint64_t *err_offset)
+{
+    GenPlan p;
+    const int rc = make_plan(prm, &p);
+    if (rc != PA_OK) return rc;
+    if (!d_edges || !d_rowptr || !d_col || !d_scratch) return PA_ERR_INVALID;
+    if (!csr_supported(prm->n)) return PA_ERR_NOT_SUPPORTED;
+    if ((reinterpret_cast<uintptr_t>(d_col) & 15u) || (reinterpret_cast<uintptr_t>(d_scratch) & 15u))
+        return PA_ERR_INVALID;
+    const CsrLayout L = csr_layout(prm->n, prm->d, p.n_edges);
+    if (scratch_bytes < L.total) return PA_ERR_CAPACITY;
+    if (err_offset) *err_offset = L.err_off;
+    if (p.id_bytes == 8)
+        return csr_enqueue_t<int64_t>(prm, p, (const int64_t *)d_edges, d_rowptr, (int64_t *)d_col,
+                                      (unsigned char *)d_scratch, L, s);
+    return csr_enqueue_t<int32_t>(prm, p, (const int32_t *)d_edges, d_rowptr, (int32_t *)d_col,
+                                  (unsigned char *)d_scratch, L, s);
+}
+
 }  // namespace pa
 
 using namespace pa;
@@ -574,20 +590,16 @@ int pa_csr_bytes(const pa_params *prm, uint64_t *rowptr_bytes, uint64_t *col_byt
 int pa_build_csr(const pa_params *prm, const void *d_edges, int64_t *d_rowptr, void *d_col,
                  void *d_scratch, uint64_t scratch_bytes, void *stream)
 {
-    GenPlan p;
-    const int rc = make_plan(prm, &p);
+    cudaStream_t s = (cudaStream_t)stream;
+    uint64_t err_off = 0;
+    const int rc = csr_enqueue(prm, d_edges, d_rowptr, d_col, d_scratch, scratch_bytes, s, &err_off);
     if (rc != PA_OK) return rc;
-    if (!d_edges || !d_rowptr || !d_col || !d_scratch) return PA_ERR_INVALID;
-    if (!csr_supported(prm->n)) return PA_ERR_NOT_SUPPORTED;
-    if ((reinterpret_cast<uintptr_t>(d_col) & 15u) || (reinterpret_cast<uintptr_t>(d_scratch) & 15u))
-        return PA_ERR_INVALID;
-    const CsrLayout L = csr_layout(prm->n, prm->d, p.n_edges);
-    if (scratch_bytes < L.total) return PA_ERR_CAPACITY;
-    if (p.id_bytes == 8)
-        return build_csr<int64_t>(prm, p, (const int64_t *)d_edges, d_rowptr, (int64_t *)d_col,
-                                  (unsigned char *)d_scratch, L, (cudaStream_t)stream);
-    return build_csr<int32_t>(prm, p, (const int32_t *)d_edges, d_rowptr, (int32_t *)d_col,
-                              (unsigned char *)d_scratch, L, (cudaStream_t)stream);
+    uint32_t herr = 0;
+    cudaError_t e = cudaMemcpyAsync(&herr, (const unsigned char *)d_scratch + err_off, 4,
+                                    cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    return (int)herr;
 }
 
 }  // extern "C"

@@ -86,6 +86,11 @@ constexpr uint64_t kStartNodesAuto = 1ull << 31;
 
 // Launch the generator kernel on `stream` into caller memory; scratch must hold
 // plan.scratch_bytes and is cleared here.
+// Queue the CSR build of a generated graph on s without waiting; the device
+// error word is at d_scratch + *err_offset once the stream has run it.
+int csr_enqueue(const pa_params *prm, const void *d_edges, int64_t *d_rowptr, void *d_col,
+                void *d_scratch, uint64_t scratch_bytes, cudaStream_t s, uint64_t *err_offset);
+
 int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, void *d_scratch,
                     cudaStream_t stream, uint32_t blocks_override,
                     const cudaEvent_t *events = nullptr);

@@ -18,8 +18,12 @@
 //      launches follow each other on the stream without a host round trip;
 //   4. sleep briefly (20 us with work in flight, else until woken).
 // Memory per request: its edge buffer plus the generation scratch of its own
-// plan, which bounds its share of the batch scratch.  Requests too large for
-// the batch kernels' 32-bit node arithmetic run as single generations.
+// plan, which bounds its share of the batch scratch; with CSR outputs also its
+// rowptr, col and CSR scratch.  The CSR of every request of a batch is queued
+// on the stream right after the batch; the CSR scratch (and the edge buffer,
+// when pairs are not kept) is freed in stream order behind it and its budget
+// returned when the batch completes.  Requests too large for the batch
+// kernels' 32-bit node arithmetic run as single generations.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -42,7 +46,10 @@ enum ReqState { RQ_QUEUED, RQ_RUNNING, RQ_DONE };
 struct Request {
     pa_params prm{};
     uint64_t n_edges = 0, edges_bytes = 0, scratch_reserve = 0;
+    uint64_t rowptr_bytes = 0, col_bytes = 0, csr_scratch = 0;   // 0 without CSR outputs
     void *edges = nullptr;
+    int64_t *rowptr = nullptr;
+    void *col = nullptr;
     int32_t status = PA_OK;
     uint32_t batch_size = 0;
     uint64_t t_submit = 0, t_start = 0, t_done = 0;
@@ -58,8 +65,8 @@ struct Pinned {
 struct Launch {
     std::vector<uint64_t> tickets;
     void *scratch = nullptr;
-    Pinned buf;            // image, then the status word at status_off
-    uint64_t status_off = 0;
+    Pinned buf;            // image; then the generation status word at status_off and
+    uint64_t status_off = 0;   // one CSR status word per request after it
     cudaEvent_t done = nullptr;
 };
 
@@ -85,7 +92,9 @@ struct pa_server {
     bool stop = false;
     pa_sched *sched = nullptr;
     std::unordered_map<uint64_t, Request> reqs;
-    std::vector<std::pair<uint64_t, void *>> to_free;     // released: ticket, buffer
+    // work for the control thread: free the buffer (if any), then return the
+    // ticket's whole budget (if the ticket is not 0)
+    std::vector<std::pair<uint64_t, void *>> to_free;
     std::deque<std::pair<uint64_t, uint64_t>> done_order;  // t_done, ticket (TTL)
     uint64_t next_ticket = 1;
     std::chrono::steady_clock::time_point t0;
@@ -120,64 +129,97 @@ Pinned get_pinned(pa_server *S, uint64_t bytes)
     return b;
 }
 
+// Queue a request's buffers for freeing and its budget for return (lock held).
+void drop_buffers(pa_server *S, uint64_t tk, Request &r)
+{
+    for (void *b : {r.edges, (void *)r.rowptr, r.col})
+        if (b) S->to_free.emplace_back(0, b);
+    S->to_free.emplace_back(tk, nullptr);
+    r.edges = nullptr;
+    r.rowptr = nullptr;
+    r.col = nullptr;
+}
+
 // Mark tickets done with `status` (lock held).  Failed requests give all their
 // memory back at once; finished ones give back their scratch share.
-void complete(pa_server *S, const std::vector<uint64_t> &tickets, int status, uint32_t batch_size)
+void complete(pa_server *S, const std::vector<uint64_t> &tickets, int status, uint32_t batch_size,
+              const uint32_t *csr_status = nullptr)
 {
     const uint64_t t = S->now();
-    for (uint64_t tk : tickets) {
+    const bool keep_pairs = (S->cfg.outputs & PA_OUT_PAIRS) != 0;
+    for (size_t q = 0; q < tickets.size(); ++q) {
+        const uint64_t tk = tickets[q];
         auto it = S->reqs.find(tk);
         if (it == S->reqs.end()) continue;
         Request &r = it->second;
+        int st = status;
+        if (st == PA_OK && csr_status) st = (int)csr_status[q];
         r.state = RQ_DONE;
-        r.status = status;
+        r.status = st;
         r.batch_size = batch_size;
         r.t_done = t;
-        if (status == PA_OK) {
+        if (st == PA_OK) {
             ++S->st.completed;
             S->st.edges_done += r.n_edges;
-            pa_sched_release(S->sched, tk, r.scratch_reserve);
+            // the generation and CSR scratch, and the pairs when not kept, are
+            // already freed on the stream
+            uint64_t give = r.scratch_reserve + r.csr_scratch;
+            if (r.col_bytes && !keep_pairs) give += r.edges_bytes;
+            pa_sched_release(S->sched, tk, give);
         } else {
             ++S->st.failed;
-            if (r.edges) S->to_free.emplace_back(tk, r.edges);
-            else pa_sched_release(S->sched, tk, UINT64_MAX);
-            r.edges = nullptr;
+            drop_buffers(S, tk, r);
         }
         S->done_order.emplace_back(t, tk);
     }
     S->cv_done.notify_all();
 }
 
-// Launch one group of admitted requests (same id width, all batchable), or one
-// single generation.  Called without the lock; `prms` and sizes were copied out
-// under it.
-void launch_group(pa_server *S, const std::vector<uint64_t> &tickets,
-                  const std::vector<pa_params> &prms, const std::vector<uint64_t> &ebytes,
-                  bool batch)
+// What the control thread needs of an admitted request (copied under the lock).
+struct Job {
+    uint64_t ticket;
+    pa_params prm;
+    uint64_t edges_bytes, rowptr_bytes, col_bytes, csr_scratch;
+};
+
+// A pool allocation; when the pool's free blocks are too fragmented, its unused
+// memory goes back to the device (after the stream drains) and the allocation
+// is tried once more.  The budget bounds what is held, not the fragmentation.
+cudaError_t pool_alloc(pa_server *S, void **p, uint64_t bytes)
 {
-    const uint32_t k = (uint32_t)tickets.size();
-    std::vector<void *> edges(k, nullptr);
-    Launch L;
-    L.tickets = tickets;
-    int rc = PA_OK;
-    cudaError_t e = cudaSuccess;
-    // The budget bounds what is held, but the pool's free blocks can be too
-    // fragmented for a large buffer: on failure, give the pool's unused memory
-    // back to the device and try once more.
-    for (int attempt = 0; attempt < 2; ++attempt) {
-        e = cudaSuccess;
-        for (uint32_t i = 0; i < k && e == cudaSuccess; ++i)
-            e = cudaMallocFromPoolAsync(&edges[i], std::max<uint64_t>(ebytes[i], 16), S->pool,
-                                        S->stream);
-        if (e == cudaSuccess || attempt == 1) break;
+    cudaError_t e = cudaMallocFromPoolAsync(p, std::max<uint64_t>(bytes, 16), S->pool, S->stream);
+    if (e != cudaSuccess) {
         (void)cudaGetLastError();
-        for (uint32_t i = 0; i < k; ++i)
-            if (edges[i]) {
-                cudaFreeAsync(edges[i], S->stream);
-                edges[i] = nullptr;
-            }
         cudaStreamSynchronize(S->stream);
         cudaMemPoolTrimTo(S->pool, 0);
+        e = cudaMallocFromPoolAsync(p, std::max<uint64_t>(bytes, 16), S->pool, S->stream);
+    }
+    return e;
+}
+
+// Launch one group of admitted requests (same id width, all batchable) as a
+// batch, or one request alone; then, with CSR outputs, every request's CSR.
+// Called without the lock.
+void launch_group(pa_server *S, const std::vector<Job> &jobs, bool batch)
+{
+    const uint32_t k = (uint32_t)jobs.size();
+    const bool csr = (S->cfg.outputs & PA_OUT_CSR) != 0;
+    const bool keep_pairs = (S->cfg.outputs & PA_OUT_PAIRS) != 0;
+    std::vector<void *> edges(k, nullptr), rowptr(k, nullptr), col(k, nullptr), cscr(k, nullptr);
+    std::vector<pa_params> prms(k);
+    std::vector<uint64_t> ebytes(k);
+    Launch L;
+    for (uint32_t i = 0; i < k; ++i) {
+        L.tickets.push_back(jobs[i].ticket);
+        prms[i] = jobs[i].prm;
+        ebytes[i] = jobs[i].edges_bytes;
+    }
+    int rc = PA_OK;
+    cudaError_t e = cudaSuccess;
+    for (uint32_t i = 0; i < k && e == cudaSuccess; ++i) {
+        e = pool_alloc(S, &edges[i], ebytes[i]);
+        if (csr && e == cudaSuccess) e = pool_alloc(S, &rowptr[i], jobs[i].rowptr_bytes);
+        if (csr && e == cudaSuccess) e = pool_alloc(S, &col[i], jobs[i].col_bytes);
     }
     if (e != cudaSuccess) rc = set_cuda_error(e);
     BatchJob J;
@@ -192,18 +234,12 @@ void launch_group(pa_server *S, const std::vector<uint64_t> &tickets,
         }
     }
     if (rc == PA_OK) {
-        e = cudaMallocFromPoolAsync(&L.scratch, scratch_bytes, S->pool, S->stream);
-        if (e != cudaSuccess) {
-            (void)cudaGetLastError();
-            cudaStreamSynchronize(S->stream);
-            cudaMemPoolTrimTo(S->pool, 0);
-            e = cudaMallocFromPoolAsync(&L.scratch, scratch_bytes, S->pool, S->stream);
-        }
+        e = pool_alloc(S, &L.scratch, scratch_bytes);
         if (e != cudaSuccess) rc = set_cuda_error(e);
     }
     if (rc == PA_OK) {
         L.status_off = (image_bytes + 15) & ~15ull;
-        L.buf = get_pinned(S, L.status_off + 16);
+        L.buf = get_pinned(S, L.status_off + 4ull * (k + 1));
         if (!L.buf.p) rc = PA_ERR_OOM;
     }
     if (rc == PA_OK && batch) {
@@ -216,7 +252,37 @@ void launch_group(pa_server *S, const std::vector<uint64_t> &tickets,
         e = cudaMemcpyAsync(L.buf.p + L.status_off,
                             (const unsigned char *)L.scratch + offsetof(GenCtl, error),
                             sizeof(uint32_t), cudaMemcpyDeviceToHost, S->stream);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming);
+        if (e != cudaSuccess) rc = set_cuda_error(e);
+    }
+    // CSR of every request, in the same stream; its scratch (and the pairs when
+    // they are not kept) is freed in stream order behind it
+    uint32_t *csr_status = reinterpret_cast<uint32_t *>(L.buf.p + L.status_off) + 1;
+    for (uint32_t i = 0; i < k && rc == PA_OK; ++i) {
+        if (!csr) {
+            csr_status[i] = PA_OK;
+            continue;
+        }
+        e = pool_alloc(S, &cscr[i], jobs[i].csr_scratch);
+        if (e != cudaSuccess) {
+            rc = set_cuda_error(e);
+            break;
+        }
+        uint64_t err_off = 0;
+        rc = csr_enqueue(&prms[i], edges[i], (int64_t *)rowptr[i], col[i], cscr[i], jobs[i].csr_scratch,
+                         S->stream, &err_off);
+        if (rc != PA_OK) break;
+        e = cudaMemcpyAsync(csr_status + i, (const unsigned char *)cscr[i] + err_off, 4,
+                            cudaMemcpyDeviceToHost, S->stream);
+        if (e == cudaSuccess) e = cudaFreeAsync(cscr[i], S->stream);
+        cscr[i] = nullptr;
+        if (e == cudaSuccess && !keep_pairs) {
+            e = cudaFreeAsync(edges[i], S->stream);
+            edges[i] = nullptr;
+        }
+        if (e != cudaSuccess) rc = set_cuda_error(e);
+    }
+    if (rc == PA_OK) {
+        e = cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventRecord(L.done, S->stream);
         if (e != cudaSuccess) rc = set_cuda_error(e);
     }
@@ -225,12 +291,17 @@ void launch_group(pa_server *S, const std::vector<uint64_t> &tickets,
         // let the stream drain before the buffers are reused or freed.
         cudaStreamSynchronize(S->stream);
         if (L.scratch) cudaFreeAsync(L.scratch, S->stream);
+        for (void *b : cscr)
+            if (b) cudaFreeAsync(b, S->stream);
         if (L.done) cudaEventDestroy(L.done);
     }
     std::lock_guard<std::mutex> lk(S->mu);
     for (uint32_t i = 0; i < k; ++i) {
-        auto it = S->reqs.find(tickets[i]);
-        if (it != S->reqs.end()) it->second.edges = edges[i];
+        auto it = S->reqs.find(jobs[i].ticket);
+        if (it == S->reqs.end()) continue;
+        it->second.edges = edges[i];
+        it->second.rowptr = (int64_t *)rowptr[i];
+        it->second.col = col[i];
     }
     ++S->st.batches;
     if (rc == PA_OK) {
@@ -238,7 +309,7 @@ void launch_group(pa_server *S, const std::vector<uint64_t> &tickets,
         return;
     }
     if (L.buf.p) S->pinned_free.push_back(L.buf);
-    complete(S, tickets, rc, k);
+    complete(S, L.tickets, rc, k);
 }
 
 void control_loop(pa_server *S)
@@ -267,7 +338,8 @@ void control_loop(pa_server *S)
             {
                 std::lock_guard<std::mutex> lk(S->mu);
                 S->pinned_free.push_back(L.buf);
-                complete(S, L.tickets, status, (uint32_t)L.tickets.size());
+                complete(S, L.tickets, status, (uint32_t)L.tickets.size(),
+                         reinterpret_cast<const uint32_t *>(L.buf.p + L.status_off) + 1);
             }
             S->inflight.pop_front();
             progressed = true;
@@ -284,8 +356,7 @@ void control_loop(pa_server *S)
                     S->done_order.pop_front();
                     auto it = S->reqs.find(tk);
                     if (it == S->reqs.end() || it->second.state != RQ_DONE) continue;
-                    if (it->second.edges) S->to_free.emplace_back(tk, it->second.edges);
-                    else pa_sched_release(S->sched, tk, UINT64_MAX);
+                    drop_buffers(S, tk, it->second);
                     S->reqs.erase(it);
                     ++S->st.expired;
                 }
@@ -296,16 +367,14 @@ void control_loop(pa_server *S)
             stopping = S->stop;
         }
         for (auto &f : frees) {
-            cudaFreeAsync(f.second, S->stream);
-            pa_sched_release(S->sched, f.first, UINT64_MAX);
+            if (f.second) cudaFreeAsync(f.second, S->stream);
+            if (f.first) pa_sched_release(S->sched, f.first, UINT64_MAX);
             progressed = true;
         }
         if (stopping && S->inflight.empty()) break;
         // 3. admission
         if (!stopping && S->inflight.size() < max_inflight) {
-            std::vector<uint64_t> t32, t64, solo;
-            std::vector<pa_params> p32, p64, psolo;
-            std::vector<uint64_t> b32, b64, bsolo;
+            std::vector<Job> j32, j64, solo;
             {
                 std::lock_guard<std::mutex> lk(S->mu);
                 const uint64_t t = S->now();
@@ -314,26 +383,17 @@ void control_loop(pa_server *S)
                     Request &r = S->reqs[adm[i]];
                     r.state = RQ_RUNNING;
                     r.t_start = t;
-                    if (!r.batchable) {
-                        solo.push_back(adm[i]);
-                        psolo.push_back(r.prm);
-                        bsolo.push_back(r.edges_bytes);
-                    } else if (r.prm.id_bits == 64) {
-                        t64.push_back(adm[i]);
-                        p64.push_back(r.prm);
-                        b64.push_back(r.edges_bytes);
-                    } else {
-                        t32.push_back(adm[i]);
-                        p32.push_back(r.prm);
-                        b32.push_back(r.edges_bytes);
-                    }
+                    const Job jb{adm[i], r.prm, r.edges_bytes, r.rowptr_bytes, r.col_bytes,
+                                 r.csr_scratch};
+                    if (!r.batchable) solo.push_back(jb);
+                    else if (r.prm.id_bits == 64) j64.push_back(jb);
+                    else j32.push_back(jb);
                 }
             }
-            if (!t32.empty()) launch_group(S, t32, p32, b32, true);
-            if (!t64.empty()) launch_group(S, t64, p64, b64, true);
-            for (size_t i = 0; i < solo.size(); ++i)
-                launch_group(S, {solo[i]}, {psolo[i]}, {bsolo[i]}, false);
-            if (!t32.empty() || !t64.empty() || !solo.empty()) progressed = true;
+            if (!j32.empty()) launch_group(S, j32, true);
+            if (!j64.empty()) launch_group(S, j64, true);
+            for (const Job &jb : solo) launch_group(S, {jb}, false);
+            if (!j32.empty() || !j64.empty() || !solo.empty()) progressed = true;
         }
         // 4. sleep
         if (!progressed) {
@@ -348,9 +408,11 @@ void control_loop(pa_server *S)
     {
         std::lock_guard<std::mutex> lk(S->mu);
         for (auto &kv : S->reqs)
-            if (kv.second.edges) cudaFreeAsync(kv.second.edges, S->stream);
+            for (void *b : {kv.second.edges, (void *)kv.second.rowptr, kv.second.col})
+                if (b) cudaFreeAsync(b, S->stream);
         S->reqs.clear();
-        for (auto &f : S->to_free) cudaFreeAsync(f.second, S->stream);
+        for (auto &f : S->to_free)
+            if (f.second) cudaFreeAsync(f.second, S->stream);
         S->to_free.clear();
         S->cv_done.notify_all();
     }
@@ -373,6 +435,8 @@ int pa_server_create(const pa_server_config *cfg, pa_server **out)
 {
     if (!cfg || !out) return PA_ERR_INVALID;
     *out = nullptr;
+    if (cfg->reserved0 != 0 || (cfg->outputs & ~(uint32_t)(PA_OUT_PAIRS | PA_OUT_CSR)) != 0)
+        return PA_ERR_INVALID;
     pa_server *S = new (std::nothrow) pa_server();
     if (!S) return PA_ERR_OOM;
     S->cfg = *cfg;
@@ -404,6 +468,7 @@ int pa_server_create(const pa_server_config *cfg, pa_server **out)
     }
     if (S->cfg.budget_bytes == 0) S->cfg.budget_bytes = (uint64_t)free_b / 4 * 3;
     if (S->cfg.aging_ns == 0) S->cfg.aging_ns = 100000000ull;
+    if (S->cfg.outputs == 0) S->cfg.outputs = PA_OUT_PAIRS;
     S->sched = pa_sched_create(S->cfg.budget_bytes, S->cfg.aging_ns, S->cfg.max_queue);
     if (!S->sched) {
         cudaMemPoolDestroy(S->pool);
@@ -431,11 +496,18 @@ int pa_server_submit(pa_server *S, const pa_params *prm, uint64_t *ticket)
     r.edges_bytes = p.edges_bytes;
     r.batchable = prm->n + 64 + 32 < (1ull << 32);
     r.scratch_reserve = scratch_reserve(*prm, r.batchable);
+    if (S->cfg.outputs & PA_OUT_CSR) {
+        rc = pa_csr_bytes(prm, &r.rowptr_bytes, &r.col_bytes, &r.csr_scratch);
+        if (rc != PA_OK) return rc;
+    }
     std::lock_guard<std::mutex> lk(S->mu);
     if (S->stop) return PA_ERR_INVALID;
     r.t_submit = S->now();
     const uint64_t tk = S->next_ticket++;
-    rc = pa_sched_submit(S->sched, tk, r.edges_bytes + r.scratch_reserve, r.t_submit);
+    rc = pa_sched_submit(S->sched, tk,
+                         r.edges_bytes + r.scratch_reserve + r.rowptr_bytes + r.col_bytes +
+                             r.csr_scratch,
+                         r.t_submit);
     if (rc != PA_OK) return rc;
     S->reqs.emplace(tk, r);
     ++S->st.submitted;
@@ -455,6 +527,9 @@ static void fill_result(const Request &r, pa_result *out)
     out->t_submit_ns = r.t_submit;
     out->t_start_ns = r.t_start;
     out->t_done_ns = r.t_done;
+    out->rowptr = r.rowptr;
+    out->col = r.col;
+    out->col_bytes = r.col ? r.col_bytes : 0;
 }
 
 int pa_server_poll(pa_server *S, uint64_t ticket, pa_result *out)
@@ -497,10 +572,10 @@ int pa_server_release(pa_server *S, uint64_t ticket)
     if (it == S->reqs.end()) return PA_ERR_NOT_FOUND;
     Request &r = it->second;
     if (r.state == RQ_RUNNING) return PA_ERR_BUSY;
-    if (r.state == RQ_QUEUED || !r.edges)
-        pa_sched_release(S->sched, ticket, UINT64_MAX);   // withdrawn, or nothing held
+    if (r.state == RQ_QUEUED)
+        pa_sched_release(S->sched, ticket, UINT64_MAX);   // withdrawn before admission
     else
-        S->to_free.emplace_back(ticket, r.edges);
+        drop_buffers(S, ticket, r);
     S->reqs.erase(it);
     ++S->st.released;
     S->cv_work.notify_one();

@@ -51,6 +51,9 @@ PA_FORMAT_BINARY = 1
 PA_FLAG_TEST_WITHHOLD_FIRST_TILE = 1 << 31
 # start_nodes: no start kernel (every node in the persistent launch)
 PA_START_NONE = (1 << 64) - 1
+# request server outputs (a mask)
+PA_OUT_PAIRS = 1
+PA_OUT_CSR = 2
 
 
 class CuppaError(RuntimeError):
@@ -114,6 +117,8 @@ class PaServerConfig(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("ttl_ns", ctypes.c_uint64),
         ("aging_ns", ctypes.c_uint64),
+        ("outputs", ctypes.c_uint32),
+        ("reserved0", ctypes.c_uint32),
     ]
 
 
@@ -127,6 +132,9 @@ class PaResult(ctypes.Structure):
         ("t_submit_ns", ctypes.c_uint64),
         ("t_start_ns", ctypes.c_uint64),
         ("t_done_ns", ctypes.c_uint64),
+        ("rowptr", ctypes.c_void_p),
+        ("col", ctypes.c_void_p),
+        ("col_bytes", ctypes.c_uint64),
     ]
 
 
@@ -546,11 +554,13 @@ class Server:
     """Continuous-batching generation server (pa_server_*)."""
 
     def __init__(self, budget_bytes: int = 0, max_batch: int = 0, max_inflight: int = 0,
-                 max_queue: int = 0, device: int = -1, ttl_ns: int = 0, aging_ns: int = 0):
+                 max_queue: int = 0, device: int = -1, ttl_ns: int = 0, aging_ns: int = 0,
+                 outputs: int = 0):
         cfg = PaServerConfig()
         check(lib().pa_server_config_init(ctypes.byref(cfg)), "pa_server_config_init")
         cfg.budget_bytes, cfg.max_batch, cfg.max_inflight = budget_bytes, max_batch, max_inflight
         cfg.max_queue, cfg.device, cfg.ttl_ns, cfg.aging_ns = max_queue, device, ttl_ns, aging_ns
+        cfg.outputs = outputs
         h = ctypes.c_void_p()
         check(lib().pa_server_create(ctypes.byref(cfg), ctypes.byref(h)), "pa_server_create")
         self._h = h
@@ -605,4 +615,15 @@ class Server:
         ts = "<i8" if id_bits == 64 else "<i4"
         arr = _DeviceArray(int(result.edges), (int(result.n_edges), 2), ts)
         return torch.as_tensor(arr, device="cuda")
+
+    @staticmethod
+    def csr_view(result: PaResult, n: int, id_bits: int):
+        """(rowptr int64 [n + 1], col [2 * n_edges]) tensors viewing a finished
+        result's CSR (server with PA_OUT_CSR; valid until the ticket is released)."""
+        torch = _torch()
+        rp = torch.as_tensor(_DeviceArray(int(result.rowptr), (n + 1,), "<i8"), device="cuda")
+        ts = "<i8" if id_bits == 64 else "<i4"
+        col = torch.as_tensor(_DeviceArray(int(result.col), (2 * int(result.n_edges),), ts),
+                              device="cuda")
+        return rp, col
 

@@ -208,6 +208,11 @@ int pa_batch_generate(const pa_params *prms, uint32_t count, void *const *d_edge
  * any thread. */
 typedef struct pa_server pa_server;
 
+/* pa_server_config.outputs: what a finished request keeps on the device (a
+ * mask; 0 = PAIRS).  With CSR the server builds each graph's undirected CSR
+ * (pa_build_csr) right after its batch, in the same stream. */
+enum { PA_OUT_PAIRS = 1, PA_OUT_CSR = 2 };
+
 typedef struct pa_server_config {
     uint64_t budget_bytes;   /* device memory for admitted requests; 0 = 3/4 of free memory */
     uint32_t max_batch;      /* requests per launch; 0 = 4096                              */
@@ -217,10 +222,13 @@ typedef struct pa_server_config {
     uint64_t ttl_ns;         /* finished results unreleased this long are freed; 0 = never */
     uint64_t aging_ns;       /* a queued request that has waited this long is not passed
                                 over by smaller ones; 0 = 100 ms                           */
+    uint32_t outputs;        /* PA_OUT_* mask; 0 = PA_OUT_PAIRS                            */
+    uint32_t reserved0;      /* must be 0                                                  */
 } pa_server_config;
 
 typedef struct pa_result {
-    const void *edges;       /* device pointer (the PAIRS layout), valid until release   */
+    const void *edges;       /* device pointer (the PAIRS layout), valid until release;
+                                NULL unless the server keeps PA_OUT_PAIRS                */
     uint64_t n_edges;
     uint64_t edges_bytes;
     int32_t status;          /* pa_status of the generation                              */
@@ -228,6 +236,9 @@ typedef struct pa_result {
     uint64_t t_submit_ns;    /* server clock: ns since pa_server_create                   */
     uint64_t t_start_ns;     /* its batch was launched                                    */
     uint64_t t_done_ns;      /* the control thread saw the batch complete                 */
+    const int64_t *rowptr;   /* with PA_OUT_CSR: int64[n + 1], valid until release        */
+    const void *col;         /* with PA_OUT_CSR: 2 * n_edges ids of id_bits width         */
+    uint64_t col_bytes;
 } pa_result;
 
 typedef struct pa_server_stats {

@@ -128,3 +128,29 @@ def test_larger_request_with_64_bit_ids(pa, cuda_ok):
         assert rc == 0
         _check_alone(pa, prm, res)
         srv.release(t)
+
+
+@pytest.mark.parametrize("outputs", ["csr", "both"])
+def test_csr_outputs_equal_alone(pa, cuda_ok, outputs):
+    """With CSR outputs every served graph's CSR equals pa_build_csr of the same
+    request generated alone; without PA_OUT_PAIRS the pair buffer is not kept,
+    and all memory returns to the budget after release."""
+    out = pa.PA_OUT_CSR | (pa.PA_OUT_PAIRS if outputs == "both" else 0)
+    rng = np.random.default_rng(3)
+    prms = _requests(pa, 40, rng, max_exp=5.0)
+    with pa.Server(budget_bytes=2 << 30, outputs=out) as srv:
+        tickets = [srv.submit(q) for q in prms]
+        for t, q in zip(tickets, prms):
+            rc, res = srv.wait(t)
+            assert rc == 0 and res.status == 0
+            want_e, _ = pa.generate(q)
+            want_rp, want_col = pa.build_csr(q, want_e)
+            rp, col = pa.Server.csr_view(res, q.n, q.id_bits)
+            assert torch.equal(rp, want_rp) and torch.equal(col, want_col)
+            if outputs == "both":
+                assert torch.equal(pa.Server.edges_view(res, q.id_bits), want_e)
+            else:
+                assert res.edges is None
+            assert srv.release(t) == 0
+        _drain(srv)
+        assert srv.stats().bytes_in_use == 0

@@ -151,6 +151,22 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(x: float, world: int, device) -> float:
+    """The largest x over all ranks (every rank takes this collective step)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank: int, steps: int, world: int, slowest_s: float) -> float:
+    """Whole-job throughput: every rank's units over the slowest rank's time."""
+    return world * units_per_rank * steps / slowest_s
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -272,15 +288,11 @@ def run_gpu(args, w):
     barrier()
     st = pa.finish(scratch, stream)
     pa.check(st.status, "timed generation")
-    ms = t_all0.elapsed_time(t_all1)
+    ms = max_over_ranks(t_all0.elapsed_time(t_all1), world, "cuda")
     fill_ms = [e[0].elapsed_time(e[1]) for e in ev]      # scratch clear + all-ones fill
     start_ms = [e[1].elapsed_time(e[2]) for e in ev]     # start kernel
     gen_ms = [e[2].elapsed_time(e[3]) for e in ev]       # persistent kernel
-    if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * E * args.steps / (ms / 1e3)
+    value = job_rate(E, args.steps, world, ms / 1e3)
 
     # ---- end to end through the C ABI: host params -> generation -> result read
     barrier()
@@ -290,12 +302,8 @@ def run_gpu(args, w):
         st = pa.finish(scratch, stream)          # stream sync + device->host result block
     t1 = time.perf_counter()
     pa.check(st.status, "e2e generation")
-    e2e_s = t1 - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": world * E * args.steps / e2e_s, "unit": "edges/s",
+    e2e_s = max_over_ranks(t1 - t0, world, "cuda")
+    e2e = {"value": job_rate(E, args.steps, world, e2e_s), "unit": "edges/s",
            "h2d_bytes_per_step": ctypes_sizeof_params(pa), "d2h_bytes_per_step": 64}
 
     if rank == 0:

@@ -305,6 +305,25 @@ def run_gpu(args, w):
     e2e_s = max_over_ranks(t1 - t0, world, "cuda")
     e2e = {"value": job_rate(E, args.steps, world, e2e_s), "unit": "edges/s",
            "h2d_bytes_per_step": ctypes_sizeof_params(pa), "d2h_bytes_per_step": 64}
+    # small graphs: the same end-to-end loop replaying a captured CUDA graph
+    # (pa_plan_*), where issuing the clear, fill and launch one by one matters
+    e2e_graph = None
+    if E < (1 << 26):
+        plan = pa.Plan(prm, edges, scratch)
+        plan.launch(stream)
+        pa.check(pa.finish(scratch, stream).status, "graph warm-up")
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            plan.launch(stream)
+            st = pa.finish(scratch, stream)
+        t1 = time.perf_counter()
+        pa.check(st.status, "graph e2e generation")
+        plan.close()
+        g_s = max_over_ranks(t1 - t0, world, "cuda")
+        e2e_graph = {"value": job_rate(E, args.steps, world, g_s), "unit": "edges/s",
+                     "ms_per_step": 1e3 * g_s / args.steps,
+                     "plain_ms_per_step": 1e3 * e2e_s / args.steps}
 
     if rank == 0:
         peak, peak_kind = load_peaks()
@@ -339,6 +358,7 @@ def run_gpu(args, w):
                                "gen_kernel": statistics.mean(gen_ms),
                                "start_split_node": u_split},
             "e2e": e2e,
+            "e2e_cuda_graph": e2e_graph,
             "gpu_launches": launches * args.steps,
             "clocks": clk.summary(),
             "device_stats": st.as_dict(),

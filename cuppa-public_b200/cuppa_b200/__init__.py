@@ -199,6 +199,10 @@ _SIGS = {
     "pa_server_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "pa_server_stats_get": (ctypes.c_int, [ctypes.c_void_p, _P(PaServerStats)]),
     "pa_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "pa_plan_create": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_uint64,
+                                      ctypes.c_void_p, ctypes.c_uint64, _P(ctypes.c_void_p)]),
+    "pa_plan_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "pa_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "pa_sched_create": (ctypes.c_void_p, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32]),
     "pa_sched_destroy": (None, [ctypes.c_void_p]),
     "pa_sched_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
@@ -513,6 +517,30 @@ class _DeviceArray:
     def __init__(self, ptr: int, shape, typestr: str):
         self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr,
                                          "data": (ptr, False), "version": 2, "strides": None}
+
+
+class Plan:
+    """A generation captured into a CUDA graph (pa_plan_*), for fixed parameters
+    and device buffers; launch() replays it."""
+
+    def __init__(self, prm: PaParams, edges, scratch):
+        h = ctypes.c_void_p()
+        check(lib().pa_plan_create(ctypes.byref(prm), ctypes.c_void_p(edges.data_ptr()),
+                                   edges.numel() * edges.element_size(),
+                                   ctypes.c_void_p(scratch.data_ptr()), scratch.numel(),
+                                   ctypes.byref(h)), "pa_plan_create")
+        self._h, self.edges, self.scratch = h, edges, scratch
+
+    def launch(self, stream=None) -> None:
+        check(lib().pa_plan_launch(self._h, ctypes.c_void_p(_stream_ptr(stream))),
+              "pa_plan_launch")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pa_plan_destroy(self._h)
+            self._h = None
+
+    __del__ = close
 
 
 class Sched:

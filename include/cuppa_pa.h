@@ -158,6 +158,20 @@ int pa_generate_noalloc(const pa_params *prm, void *d_edges, uint64_t edges_byte
 int pa_generate_trace(const pa_params *prm, const void *d_scratch, uint64_t *out,
                       uint32_t max_samples, uint32_t *count, void *stream);
 
+/* ---- captured generations (CUDA graphs) --------------------------------------- */
+/* For small graphs, issuing the scratch clear, the sentinel fill and the kernel
+ * launch one by one costs about as much as the GPU work.  A plan captures that
+ * sequence once, for fixed parameters and buffers, into a CUDA graph;
+ * pa_plan_launch replays it on `stream` with one graph launch and writes what
+ * pa_generate would.  The buffers must outlive the plan and must not be used by
+ * anything else while a replay runs; read the status with
+ * pa_generate_finish(d_scratch, ...).  No counterpart in the reference. */
+typedef struct pa_plan pa_plan;
+int pa_plan_create(const pa_params *prm, void *d_edges, uint64_t edges_bytes, void *d_scratch,
+                   uint64_t scratch_bytes, pa_plan **out);
+int pa_plan_launch(pa_plan *plan, void *stream);
+int pa_plan_destroy(pa_plan *plan);
+
 /* ---- post-processing ------------------------------------------------------ */
 /* Sort every node's d pairs by dst in place (or into d_out): the canonical edge
  * list -- all (u, v) with u > v sorted by (u, v). */

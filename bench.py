@@ -479,7 +479,9 @@ def run_served(args):
                            seed_mode=pa.PA_SEED_CLIQUE) for r in reqs]
     tickets = queue.Queue()
     lat, edges_done, statuses = [], 0, []
-    with pa.Server(budget_bytes=budget) as srv, ClockSampler(0) as clk:
+    outputs = {"pairs": pa.PA_OUT_PAIRS, "csr": pa.PA_OUT_CSR,
+               "both": pa.PA_OUT_PAIRS | pa.PA_OUT_CSR}[args.serve_outputs]
+    with pa.Server(budget_bytes=budget, outputs=outputs) as srv, ClockSampler(0) as clk:
         # warm-up: a few requests, waited for and released
         for q in prms[: args.warmup]:
             t = srv.submit(q)
@@ -529,11 +531,13 @@ def run_served(args):
         "config": {"workload": f"Poisson {args.rate:g} req/s for {args.serve_seconds:g} s: "
                                "n=round(10^U(4,8)), d=U{2..16}, p=U(0.2,0.8), int32, clique seed",
                    "requests": len(reqs), "budget_gb": budget / 1e9,
-                   "output": "edge list (PAIRS) kept on the device until released"},
+                   "output": {"pairs": "edge list (PAIRS)", "csr": "undirected CSR",
+                              "both": "edge list and undirected CSR"}[args.serve_outputs]
+                             + " kept on the device until released"},
         "p50_ms": pct(50), "p99_ms": pct(99), "max_ms": lat_sorted[-1],
         "requests_per_s": len(reqs) / span_s, "all_ok": ok, "server_stats": st,
         "statuses": {str(c): statuses.count(c) for c in sorted(set(statuses))},
-        "gpu_launches": 2 * st["batches"],
+        "gpu_launches": st["batches"] * 2 + (st["completed"] * 11 if outputs & pa.PA_OUT_CSR else 0),
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -561,6 +565,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=5.0, help="served: arrival window")
     ap.add_argument("--rate", type=float, default=2000.0, help="served: mean requests/s")
     ap.add_argument("--serve-budget-gb", type=float, default=150.0, help="served: HBM budget")
+    ap.add_argument("--serve-outputs", choices=["pairs", "csr", "both"], default="csr",
+                    help="served: what each finished request keeps on the device")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

@@ -168,19 +168,31 @@ __global__ void out_part_kernel(const Id *E, const int64_t *rowptr, Id *col, uin
     const uint32_t g = lane / d, i = lane - g * d;
     const bool used = lane < G * d;
     const uint64_t rows = n - (d + 1);
-    for (uint64_t r0 = w0 * G; r0 < rows; r0 += warps * G) {
-        const uint64_t row = r0 + g;
-        const bool act = used && row < rows;
-        Id dst = 0;
-        if (act) dst = E[2 * (seed_edges + row * d + i) + 1];
-        uint32_t rank = 0;
-        for (uint32_t j = 0; j < d; ++j) {
-            const Id o = __shfl_sync(kFull, dst, (g * d + j) & 31u);
-            rank += (o < dst) ? 1u : 0u;
+    // four row groups per warp per step, their loads issued together
+    constexpr int R = 4;
+    for (uint64_t r0 = w0 * G; r0 < rows; r0 += R * warps * G) {
+        Id dst[R];
+        int64_t rp[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+            const uint64_t row = r0 + q * warps * G + g;
+            const bool act = used && row < rows;
+            dst[q] = act ? E[2 * (seed_edges + row * d + i) + 1] : (Id)0;
+            rp[q] = act ? rowptr[row + d + 1] : 0;
         }
-        if (act) {
-            const uint64_t pos = (uint64_t)rowptr[row + d + 1] + rank;
-            if (pos < col_len) col[pos] = dst;
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+            const uint64_t row = r0 + q * warps * G + g;
+            const bool act = used && row < rows;
+            uint32_t rank = 0;
+            for (uint32_t j = 0; j < d; ++j) {
+                const Id o = __shfl_sync(kFull, dst[q], (g * d + j) & 31u);
+                rank += (o < dst[q]) ? 1u : 0u;
+            }
+            if (act) {
+                const uint64_t pos = (uint64_t)rp[q] + rank;
+                if (pos < col_len) col[pos] = dst[q];
+            }
         }
     }
 }
@@ -293,21 +305,33 @@ __global__ void __launch_bounds__(kRadixThreads) radix_scatter_kernel(const void
     const uint64_t tb = t * kRadixTile;
     const uint32_t tcount = (uint32_t)min((uint64_t)kRadixTile, n_items - tb);
     const uint32_t wo = warp * (kRadixRounds * 32);
-    // 1. stable ranks within the warp's items (in order, 32 per round)
-    for (uint32_t r = 0; r < kRadixRounds; ++r) {
-        const uint32_t k = wo + r * 32 + lane;
-        const bool valid = k < tcount;
-        uint32_t dg = NB + lane;   // unique for lanes past the end
-        if (valid) dg = (uint32_t)(radix_item<Id, First>(src, tb + k, n, err) >> (32 + shift)) & MASK;
-        const uint32_t peers = __match_any_sync(kFull, dg);
-        const uint32_t leader = __ffs(peers) - 1;
-        uint32_t old = 0;
-        if (valid && lane == leader) {
-            old = S.wcnt[warp][dg];
-            S.wcnt[warp][dg] = old + __popc(peers);
+    // 1. stable ranks within the warp's items (in order, 32 per round); the
+    // loads of kBatch rounds are issued together
+    constexpr uint32_t kBatch = 8;
+    for (uint32_t r0 = 0; r0 < kRadixRounds; r0 += kBatch) {
+        uint32_t dgs[kBatch];
+#pragma unroll
+        for (uint32_t q = 0; q < kBatch; ++q) {
+            const uint32_t k = wo + (r0 + q) * 32 + lane;
+            dgs[q] = k < tcount
+                         ? (uint32_t)(radix_item<Id, First>(src, tb + k, n, err) >> (32 + shift)) & MASK
+                         : NB + lane;   // unique for lanes past the end
         }
-        old = __shfl_sync(kFull, old, leader);
-        if (valid) S.lrank[k] = (uint16_t)(old + __popc(peers & lt));
+#pragma unroll
+        for (uint32_t q = 0; q < kBatch; ++q) {
+            const uint32_t k = wo + (r0 + q) * 32 + lane;
+            const bool valid = k < tcount;
+            const uint32_t dg = dgs[q];
+            const uint32_t peers = __match_any_sync(kFull, dg);
+            const uint32_t leader = __ffs(peers) - 1;
+            uint32_t old = 0;
+            if (valid && lane == leader) {
+                old = S.wcnt[warp][dg];
+                S.wcnt[warp][dg] = old + __popc(peers);
+            }
+            old = __shfl_sync(kFull, old, leader);
+            if (valid) S.lrank[k] = (uint16_t)(old + __popc(peers & lt));
+        }
     }
     __syncthreads();
     // 2. per digit (thread j owns digits j*PER .. j*PER+PER-1): warp bases in
@@ -345,12 +369,20 @@ __global__ void __launch_bounds__(kRadixThreads) radix_scatter_kernel(const void
     }
     __syncthreads();
     // 3. the tile's items into shared memory in digit order (read again, from L2)
-    for (uint32_t r = 0; r < kRadixRounds; ++r) {
-        const uint32_t k = wo + r * 32 + lane;
-        if (k < tcount) {
-            const unsigned long long it = radix_item<Id, First>(src, tb + k, n, err);
-            const uint32_t dg = (uint32_t)(it >> (32 + shift)) & MASK;
-            S.stage[S.lstart[dg] + S.wcnt[warp][dg] + S.lrank[k]] = it;
+    for (uint32_t r0 = 0; r0 < kRadixRounds; r0 += kBatch) {
+        unsigned long long its[kBatch];
+#pragma unroll
+        for (uint32_t q = 0; q < kBatch; ++q) {
+            const uint32_t k = wo + (r0 + q) * 32 + lane;
+            its[q] = k < tcount ? radix_item<Id, First>(src, tb + k, n, err) : 0ull;
+        }
+#pragma unroll
+        for (uint32_t q = 0; q < kBatch; ++q) {
+            const uint32_t k = wo + (r0 + q) * 32 + lane;
+            if (k < tcount) {
+                const uint32_t dg = (uint32_t)(its[q] >> (32 + shift)) & MASK;
+                S.stage[S.lstart[dg] + S.wcnt[warp][dg] + S.lrank[k]] = its[q];
+            }
         }
     }
     __syncthreads();
@@ -402,13 +434,23 @@ __global__ void in_sorted_kernel(const unsigned long long *items, uint64_t n_ite
                                  uint32_t d, uint64_t seed_edges, const int64_t *seed_pre, Id *col,
                                  uint64_t col_len)
 {
+    // four items per thread per step, their loads issued together
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_items; i += stride) {
-        const unsigned long long it = items[i];
-        const uint64_t v = it >> 32;
-        if (v >= n) continue;
-        const uint64_t pos = outprefix(v + 1, d, seed_edges, seed_pre) + i;
-        if (pos < col_len) col[pos] = (Id)(it & 0xffffffffull);
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n_items; i0 += 4 * stride) {
+        unsigned long long its[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint64_t i = i0 + q * stride;
+            its[q] = i < n_items ? items[i] : ~0ull;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint64_t i = i0 + q * stride;
+            const uint64_t v = its[q] >> 32;
+            if (i >= n_items || v >= n) continue;
+            const uint64_t pos = outprefix(v + 1, d, seed_edges, seed_pre) + i;
+            if (pos < col_len) col[pos] = (Id)(its[q] & 0xffffffffull);
+        }
     }
 }
 

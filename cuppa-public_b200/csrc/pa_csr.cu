@@ -227,9 +227,9 @@ __global__ void seed_out_kernel(const Id *E, uint64_t seed_edges, uint32_t d, ui
 // time, with __match_any_sync for equal digits and per-warp counters in shared
 // memory, then the warps' counts are prefixed per digit -- and writes it.
 // ---------------------------------------------------------------------------
-constexpr uint32_t kRadixThreads = 256, kRadixWarps = kRadixThreads / 32;
+constexpr uint32_t kRadixThreads = 512, kRadixWarps = kRadixThreads / 32;
 constexpr uint32_t kRadixBuckets = 512;   // the widest digit: 9 bits
-constexpr uint32_t kRadixRounds = 32;   // items per lane per tile
+constexpr uint32_t kRadixRounds = 16;   // items per lane per tile
 constexpr uint32_t kRadixTile = kRadixThreads * kRadixRounds;
 constexpr unsigned long long kBadKey = 0xffffffffull;   // sorts after every node id
 
@@ -281,19 +281,20 @@ template <uint32_t NB>
 struct RadixSmem {
     unsigned long long stage[kRadixTile];
     unsigned long long goff[NB];                  // this tile's global offset per digit
-    uint32_t wcnt[kRadixWarps][NB];               // per-warp digit counts, then bases
+    uint16_t wcnt[kRadixWarps][NB];               // per-warp digit counts, then bases (<= tile)
     uint32_t lstart[NB];                          // digit start within the tile
     uint16_t lrank[kRadixTile];                   // rank within the warp's items of its digit
 };
 
 template <typename Id, bool First, uint32_t DB>
-__global__ void __launch_bounds__(kRadixThreads) radix_scatter_kernel(const void *src,
+__global__ void __launch_bounds__(kRadixThreads, 2) radix_scatter_kernel(const void *src,
                                                                       unsigned long long *dst,
                                                                       uint64_t n_items, uint32_t shift,
                                                                       uint64_t n, const int64_t *offs,
                                                                       uint64_t n_tiles, uint32_t *err)
 {
-    constexpr uint32_t NB = 1u << DB, MASK = NB - 1, PER = NB / kRadixThreads;
+    constexpr uint32_t NB = 1u << DB, MASK = NB - 1;
+    constexpr uint32_t PER = NB > kRadixThreads ? NB / kRadixThreads : 1;   // digits per thread
     extern __shared__ __align__(16) unsigned char smem_raw[];
     RadixSmem<NB> &S = *reinterpret_cast<RadixSmem<NB> *>(smem_raw);
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -327,7 +328,7 @@ __global__ void __launch_bounds__(kRadixThreads) radix_scatter_kernel(const void
             uint32_t old = 0;
             if (valid && lane == leader) {
                 old = S.wcnt[warp][dg];
-                S.wcnt[warp][dg] = old + __popc(peers);
+                S.wcnt[warp][dg] = (uint16_t)(old + __popc(peers));
             }
             old = __shfl_sync(kFull, old, leader);
             if (valid) S.lrank[k] = (uint16_t)(old + __popc(peers & lt));
@@ -341,15 +342,18 @@ __global__ void __launch_bounds__(kRadixThreads) radix_scatter_kernel(const void
 #pragma unroll
     for (uint32_t q = 0; q < PER; ++q) {
         const uint32_t dg = threadIdx.x * PER + q;
-        uint32_t acc = 0;
-        for (uint32_t w = 0; w < kRadixWarps; ++w) {
-            const uint32_t c = S.wcnt[w][dg];
-            S.wcnt[w][dg] = acc;
-            acc += c;
+        tot[q] = 0;
+        if (dg < NB) {
+            uint32_t acc = 0;
+            for (uint32_t w = 0; w < kRadixWarps; ++w) {
+                const uint32_t c = S.wcnt[w][dg];
+                S.wcnt[w][dg] = (uint16_t)acc;
+                acc += c;
+            }
+            tot[q] = acc;
+            S.goff[dg] = (unsigned long long)offs[(uint64_t)dg * n_tiles + t];
         }
-        tot[q] = acc;
-        mine += acc;
-        S.goff[dg] = (unsigned long long)offs[(uint64_t)dg * n_tiles + t];
+        mine += tot[q];
     }
     uint32_t x = mine;
 #pragma unroll
@@ -364,7 +368,8 @@ __global__ void __launch_bounds__(kRadixThreads) radix_scatter_kernel(const void
     for (uint32_t w = 0; w < warp; ++w) run += s_wsum[w];
 #pragma unroll
     for (uint32_t q = 0; q < PER; ++q) {
-        S.lstart[threadIdx.x * PER + q] = run;
+        const uint32_t dg = threadIdx.x * PER + q;
+        if (dg < NB) S.lstart[dg] = run;
         run += tot[q];
     }
     __syncthreads();

@@ -95,3 +95,26 @@ def tune(n: int, d: int, p: float = 0.5, id_bits: int = 32, reps: int = 3, table
     if path:
         save(t, path)
     return best, times
+
+
+def main(argv=None):
+    """python -m cuppa_b200.autotune [--out PATH] [--log2n 12 16 20 24] [--d 2 4 8 16 32]
+    tunes every (2^e, d) int32 bucket and writes the table."""
+    import argparse
+    ap = argparse.ArgumentParser(description="launch-shape autotuner")
+    ap.add_argument("--out", default=DEFAULT_TABLE)
+    ap.add_argument("--log2n", type=int, nargs="+", default=[12, 16, 20, 24])
+    ap.add_argument("--d", type=int, nargs="+", default=[2, 4, 8, 16, 32])
+    ap.add_argument("--id-bits", type=int, default=32)
+    ap.add_argument("--reps", type=int, default=3)
+    args = ap.parse_args(argv)
+    table = load(args.out)
+    for e in args.log2n:
+        for d in args.d:
+            best, times = tune(2 ** e, d, 0.5, args.id_bits, reps=args.reps, table=table, path=None)
+            print(bucket(2 ** e, d, args.id_bits), best, [round(t, 4) for t, _ in times], flush=True)
+    save(table, args.out)
+
+
+if __name__ == "__main__":
+    main()

@@ -168,31 +168,19 @@ __global__ void out_part_kernel(const Id *E, const int64_t *rowptr, Id *col, uin
     const uint32_t g = lane / d, i = lane - g * d;
     const bool used = lane < G * d;
     const uint64_t rows = n - (d + 1);
-    // four row groups per warp per step, their loads issued together
-    constexpr int R = 4;
-    for (uint64_t r0 = w0 * G; r0 < rows; r0 += R * warps * G) {
-        Id dst[R];
-        int64_t rp[R];
-#pragma unroll
-        for (int q = 0; q < R; ++q) {
-            const uint64_t row = r0 + q * warps * G + g;
-            const bool act = used && row < rows;
-            dst[q] = act ? E[2 * (seed_edges + row * d + i) + 1] : (Id)0;
-            rp[q] = act ? rowptr[row + d + 1] : 0;
+    for (uint64_t r0 = w0 * G; r0 < rows; r0 += warps * G) {
+        const uint64_t row = r0 + g;
+        const bool act = used && row < rows;
+        Id dst = 0;
+        if (act) dst = E[2 * (seed_edges + row * d + i) + 1];
+        uint32_t rank = 0;
+        for (uint32_t j = 0; j < d; ++j) {
+            const Id o = __shfl_sync(kFull, dst, (g * d + j) & 31u);
+            rank += (o < dst) ? 1u : 0u;
         }
-#pragma unroll
-        for (int q = 0; q < R; ++q) {
-            const uint64_t row = r0 + q * warps * G + g;
-            const bool act = used && row < rows;
-            uint32_t rank = 0;
-            for (uint32_t j = 0; j < d; ++j) {
-                const Id o = __shfl_sync(kFull, dst[q], (g * d + j) & 31u);
-                rank += (o < dst[q]) ? 1u : 0u;
-            }
-            if (act) {
-                const uint64_t pos = (uint64_t)rp[q] + rank;
-                if (pos < col_len) col[pos] = dst[q];
-            }
+        if (act) {
+            const uint64_t pos = (uint64_t)rowptr[row + d + 1] + rank;
+            if (pos < col_len) col[pos] = dst;
         }
     }
 }
@@ -220,12 +208,14 @@ __global__ void seed_out_kernel(const Id *E, uint64_t seed_edges, uint32_t d, ui
 // (number of items with key < x), read off the run boundaries.  No atomics on
 // the node range, no per-row sorting, no special path for hub rows.
 //
-// A pass sorts 8 key bits: a histogram kernel counts the digits of every tile
-// of 8192 items into a digit-major table, an exclusive scan of the table gives
-// each (digit, tile) its output offset, and the scatter kernel ranks every item
-// within its tile stably -- each warp walks its 1024 items in order, 32 at a
-// time, with __match_any_sync for equal digits and per-warp counters in shared
-// memory, then the warps' counts are prefixed per digit -- and writes it.
+// A pass sorts 8 or 9 key bits: a histogram kernel counts the digits of every
+// tile of 8192 items into a digit-major table, an exclusive scan of the table
+// gives each (digit, tile) its output offset, and the scatter kernel ranks every
+// item within its tile stably -- each of 16 warps walks its 512 items in order,
+// 32 at a time, with __match_any_sync for equal digits and 16-bit per-warp
+// counters in shared memory, then the warps' counts are prefixed per digit --
+// stages the tile in shared memory in digit order and writes each digit's run
+// contiguously.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kRadixThreads = 512, kRadixWarps = kRadixThreads / 32;
 constexpr uint32_t kRadixBuckets = 512;   // the widest digit: 9 bits
@@ -418,43 +408,25 @@ __global__ void seed_prefix_kernel(const uint32_t *seed_out, uint32_t d, int64_t
     }
 }
 
-// rowptr[x] = outprefix(x) + #items with key < x, from the sorted keys: item i
-// writes every x in (key(i-1), key(i)]; i = n_items closes the range up to n.
-__global__ void rowptr_kernel(const unsigned long long *items, uint64_t n_items, uint64_t n,
-                              uint32_t d, uint64_t seed_edges, const int64_t *seed_pre,
-                              int64_t *rowptr)
-{
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n_items; i += stride) {
-        const uint64_t hi = i < n_items ? min((uint64_t)(items[i] >> 32), n) : n;
-        const uint64_t lo = i > 0 ? min((uint64_t)(items[i - 1] >> 32), n) + 1 : 0;
-        for (uint64_t x = lo; x <= hi && x <= n; ++x)
-            rowptr[x] = (int64_t)(outprefix(x, d, seed_edges, seed_pre) + i);
-    }
-}
-
-// In parts: sorted item i (key v, value u) to col[outprefix(v + 1) + i].
+// One pass over the sorted items: in part entry i (key v, value u) goes to
+// col[outprefix(v + 1) + i], and rowptr[x] = outprefix(x) + #items with key < x
+// is written for every x in (key(i-1), key(i)] (i = n_items closes the range up
+// to n; keys >= n -- only after an input error -- count as n).
 template <typename Id>
 __global__ void in_sorted_kernel(const unsigned long long *items, uint64_t n_items, uint64_t n,
                                  uint32_t d, uint64_t seed_edges, const int64_t *seed_pre, Id *col,
-                                 uint64_t col_len)
+                                 uint64_t col_len, int64_t *rowptr)
 {
-    // four items per thread per step, their loads issued together
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n_items; i0 += 4 * stride) {
-        unsigned long long its[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const uint64_t i = i0 + q * stride;
-            its[q] = i < n_items ? items[i] : ~0ull;
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const uint64_t i = i0 + q * stride;
-            const uint64_t v = its[q] >> 32;
-            if (i >= n_items || v >= n) continue;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n_items; i += stride) {
+        const unsigned long long it = i < n_items ? items[i] : ~0ull;
+        const uint64_t v = i < n_items ? min((uint64_t)(it >> 32), n) : n;
+        const uint64_t lo = i > 0 ? min((uint64_t)(items[i - 1] >> 32), n) + 1 : 0;
+        for (uint64_t x = lo; x <= v && x <= n; ++x)
+            rowptr[x] = (int64_t)(outprefix(x, d, seed_edges, seed_pre) + i);
+        if (i < n_items && v < n) {
             const uint64_t pos = outprefix(v + 1, d, seed_edges, seed_pre) + i;
-            if (pos < col_len) col[pos] = (Id)(its[q] & 0xffffffffull);
+            if (pos < col_len) col[pos] = (Id)(it & 0xffffffffull);
         }
     }
 }
@@ -582,10 +554,9 @@ int csr_enqueue_t(const pa_params *prm, const GenPlan &p, const Id *E, int64_t *
                      : radix_pass<Id, 8>(q == 0, src, dst, m, shift, n, table, scratch, L, err, s);
         if (rc != PA_OK) return rc;
     }
-    rowptr_kernel<<<grid_for(m + 1, 256), 256, 0, s>>>(A, m, n, d, p.seed_edges, seed_pre, rowptr);
     const uint64_t col_len = 2 * m;
-    in_sorted_kernel<Id><<<grid_for(m, 256), 256, 0, s>>>(A, m, n, d, p.seed_edges, seed_pre, col,
-                                                          col_len);
+    in_sorted_kernel<Id><<<grid_for(m + 1, 256), 256, 0, s>>>(A, m, n, d, p.seed_edges, seed_pre, col,
+                                                              col_len, rowptr);
     out_part_kernel<Id><<<grid_for(n * d, 256), 256, 0, s>>>(E, rowptr, col, n, d, p.seed_edges,
                                                              col_len);
     e = cudaGetLastError();

@@ -194,6 +194,67 @@ int orc_generate(uint64_t n, uint32_t d, double p, uint64_t seed, int seed_mode,
     return 0;
 }
 
+/*
+ * Repeated-nodes Barabasi-Albert (the reference's -A sba,
+ * src/PA/SPA/SerialBA.cpp:68-186): node u picks d distinct targets uniformly
+ * from the endpoint list of all earlier edges -- the seed block (node i < d
+ * repeated 2d times) followed, per node w = d, d+1, ..., by [target_0, w,
+ * target_1, w, ...] -- so a draw is R uniform in [0, Z_u), Z_u = 2d^2 +
+ * 2d(u - d), decoded as: R < 2d^2 -> node R / 2d; else r = R - 2d^2, w = d +
+ * r / 2d, q = r % 2d -> q odd: w itself, q even: the target in slot q/2 of w.
+ * Node d's targets are 0..d-1 (the reference's initial set), which is the
+ * STAR_REF seed row.  PHILOX: R = mulhi64(w1:w0, Z_u) of
+ * Philox(ctr = (u_lo, u_hi, i, r)); MT_REF: R = U % Z_u from the reference's
+ * MT19937-64 stream, one draw per try, nodes in order.
+ */
+static int64_t ba_endpoint(uint64_t R, uint32_t d, const int64_t *G)
+{
+    const uint64_t seed_block = 2ull * d * d;
+    if (R < seed_block) return (int64_t)(R / (2ull * d));
+    const uint64_t r = R - seed_block;
+    const uint64_t w = d + r / (2ull * d);
+    const uint64_t q = r % (2ull * d);
+    return (q & 1) ? (int64_t)w : G[w * d + q / 2];
+}
+
+int orc_generate_ba(uint64_t n, uint32_t d, uint64_t seed, int rng, int64_t *G,
+                    uint64_t *retries_out)
+{
+    if (d == 0 || n < (uint64_t)d + 1 || G == NULL) return -1;
+    if (rng != ORC_RNG_PHILOX && rng != ORC_RNG_MT_REF) return -1;
+    for (uint64_t v = 0; v <= d; ++v)
+        for (uint32_t k = 0; k < d; ++k) G[v * d + k] = seed_slot(v, k, d, ORC_SEED_STAR_REF);
+    uint64_t retries = 0;
+    const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    mt64 m;
+    mt64_seed(&m, seed);
+    for (uint64_t u = (uint64_t)d + 1; u < n; ++u) {
+        int64_t *row = G + u * d;
+        const uint64_t Z = 2ull * d * d + 2ull * d * (u - d);
+        for (uint32_t i = 0; i < d; ++i) {
+            for (uint32_t r = 0;; ++r) {
+                uint64_t R;
+                if (rng == ORC_RNG_PHILOX) {
+                    const uint32_t ctr[4] = {(uint32_t)u, (uint32_t)(u >> 32), i, r};
+                    uint32_t w[4];
+                    orc_philox4x32_10(ctr, key, w);
+                    R = mulhi64(((uint64_t)w[1] << 32) | w[0], Z);
+                } else {
+                    R = mt64_next(&m) % Z;
+                }
+                const int64_t cand = ba_endpoint(R, d, G);
+                int dup = 0;
+                for (uint32_t j = 0; j < i; ++j)
+                    if (row[j] == cand) { dup = 1; break; }
+                if (!dup) { row[i] = cand; break; }
+                ++retries;
+            }
+        }
+    }
+    if (retries_out) *retries_out = retries;
+    return 0;
+}
+
 /* ------------------------------------------------------------------------ */
 /* Output forms                                                              */
 /* ------------------------------------------------------------------------ */

@@ -64,6 +64,15 @@ int orc_generate(uint64_t n, uint32_t d, double p, uint64_t seed, int seed_mode,
                  int rng, int64_t *G, uint64_t *retries_out);
 
 /*
+ * The repeated-nodes Barabasi-Albert model (the reference's -A sba,
+ * src/PA/SPA/SerialBA.cpp:68-186) in the same slot array: STAR_REF seed rows,
+ * then node u's d distinct targets drawn uniformly from the endpoints of all
+ * earlier edges.  rng as for orc_generate (MT_REF: the reference's own stream).
+ */
+int orc_generate_ba(uint64_t n, uint32_t d, uint64_t seed, int rng, int64_t *G,
+                    uint64_t *retries_out);
+
+/*
  * Edge list in the GPU generator's PAIRS layout: the canonical seed edges
  * (u > v, sorted), then rows d+1..n-1 in slot (generation) order.
  * pairs has 2*orc_edge_count() entries (src, dst interleaved).

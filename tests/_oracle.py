@@ -16,6 +16,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 LIB = os.path.join(ORACLE_DIR, "liboracle.so")
 REF_SCM = os.path.join(ORACLE_DIR, "_ref", "scm_ref")
+REF_SBA = os.path.join(ORACLE_DIR, "_ref", "sba_ref")
 
 SEED_STAR_REF = 0
 SEED_CLIQUE = 1
@@ -42,6 +43,8 @@ def lib() -> ctypes.CDLL:
         L.orc_edge_count.restype = _u64
         L.orc_generate.argtypes = [_u64, _u32, ctypes.c_double, _u64, _i, _i, _vp, _vp]
         L.orc_generate.restype = _i
+        L.orc_generate_ba.argtypes = [_u64, _u32, _u64, _i, _vp, _vp]
+        L.orc_generate_ba.restype = _i
         for f in ("orc_pairs_slot_order", "orc_pairs_canonical", "orc_degrees"):
             getattr(L, f).argtypes = [_u64, _u32, _i, _vp, _vp]
         L.orc_csr.argtypes = [_u64, _u32, _i, _vp, _vp, _vp]
@@ -85,6 +88,17 @@ def generate(n: int, d: int, p: float, seed: int, seed_mode: int = SEED_CLIQUE,
     rc = lib().orc_generate(n, d, p, seed, seed_mode, rng, G.ctypes.data, ctypes.byref(r))
     if rc != 0:
         raise ValueError(f"oracle rejected n={n} d={d} p={p}")
+    G = G.reshape(n, d)
+    return (G, int(r.value)) if with_retries else G
+
+
+def generate_ba(n: int, d: int, seed: int, rng: int = RNG_PHILOX, with_retries: bool = False):
+    """Slot array G[n][d] (int64) of the repeated-nodes BA model (STAR_REF seed)."""
+    G = np.empty(n * d, dtype=np.int64)
+    r = ctypes.c_uint64()
+    rc = lib().orc_generate_ba(n, d, seed, rng, G.ctypes.data, ctypes.byref(r))
+    if rc != 0:
+        raise ValueError(f"oracle rejected BA n={n} d={d}")
     G = G.reshape(n, d)
     return (G, int(r.value)) if with_retries else G
 

@@ -11,11 +11,15 @@ Two kinds of fixture:
    MT19937-64 with the default 5489 and its seed graph is the star seed, so these
    runs are deterministic.  They pin the oracle's MT_REF mode exactly and are the
    samples for the statistical comparison of the Philox generator.
+   oracle/_ref/sba_ref is the reference's repeated-nodes BA (-A sba,
+   src/PA/SPA/SerialBA.cpp, same seed 5489); its "Degree,Count" CSVs
+   (src/PA/SPA/PAHelper.hpp:69-147) pin the oracle's BA model in MT_REF mode.
 2. Oracle digests.  FNV-1a 64 of the oracle's Philox-mode edge lists (slot
    order and canonical, int64 little-endian) for a fixed list of shapes, plus one
    tiny full edge list.  They pin the oracle itself across edits.
 
-Needs the reference tree only for part 1 (scm_ref must already be built).
+Needs the reference tree only for part 1 (scm_ref and sba_ref must already be
+built).
 """
 from __future__ import annotations
 
@@ -39,6 +43,16 @@ SCM_RUNS = [
     (20000, 8, 0.5), (5000, 1, 0.5), (30000, 16, 0.3), (10000, 32, 0.5),
     (3000, 2, 1.0), (1000000, 4, 0.2), (1000000, 4, 0.5), (1000000, 4, 0.8),
 ]
+
+# (n, M) runs of the reference sba.
+SBA_RUNS = [
+    (20000, 4), (5000, 1), (10000, 8), (3000, 32), (50000, 2), (20000, 16),
+    (1000000, 4),
+]
+
+# Philox-mode BA digests: (n, d, seed).
+BA_DIGEST_CASES = [(100000, 4, 42), (20000, 16, 7), (5000, 1, 3), (5000, 32, 5),
+                   (4000, 7, 2 ** 40 + 17)]
 
 # Philox-mode digests: (n, d, p, seed, seed_mode).
 DIGEST_CASES = [
@@ -75,6 +89,39 @@ def scm_fixtures():
                                 "star seed", "runs": index}, f, indent=1)
 
 
+def sba_fixtures():
+    if not os.path.exists(orc.REF_SBA):
+        raise SystemExit(f"{orc.REF_SBA} missing: run `make -C oracle ref` first")
+    outdir = os.path.join(HERE, "sba_dd")
+    os.makedirs(outdir, exist_ok=True)
+    index = []
+    for n, m in SBA_RUNS:
+        name = f"sba_n{n}_m{m}.csv"
+        with tempfile.TemporaryDirectory() as td:
+            subprocess.run([orc.REF_SBA, str(n), str(m), td, name], check=True, cwd=td,
+                           stdout=subprocess.DEVNULL)
+            with open(os.path.join(td, name)) as f:
+                text = f.read()
+        with open(os.path.join(outdir, name), "w") as f:
+            f.write(text)
+        index.append({"n": n, "m": m, "file": f"sba_dd/{name}"})
+    with open(os.path.join(HERE, "sba_dd.json"), "w") as f:
+        json.dump({"generator": "reference -A sba (SerialBA.cpp), MT19937-64 seed 5489",
+                   "runs": index}, f, indent=1)
+
+
+def ba_digest_fixtures():
+    cases = []
+    for n, d, seed in BA_DIGEST_CASES:
+        G, retries = orc.generate_ba(n, d, seed, orc.RNG_PHILOX, with_retries=True)
+        slot = orc.pairs_slot_order(G, orc.SEED_STAR_REF)
+        cases.append({"n": n, "d": d, "seed": seed, "edges": int(slot.shape[0]),
+                      "retries": retries, "fnv_slot_i64": f"{orc.fnv1a64(slot):016x}"})
+    with open(os.path.join(HERE, "ba_philox_digests.json"), "w") as f:
+        json.dump({"digest": "FNV-1a 64 over little-endian (src, dst) pairs, slot order",
+                   "cases": cases}, f, indent=1)
+
+
 def digest_fixtures():
     cases = []
     for n, d, p, seed, mode in DIGEST_CASES:
@@ -100,5 +147,7 @@ def digest_fixtures():
 
 if __name__ == "__main__":
     scm_fixtures()
+    sba_fixtures()
     digest_fixtures()
+    ba_digest_fixtures()
     print("fixtures written to", HERE)

@@ -7,9 +7,11 @@
 * MT_REF mode (the reference's own RNG and draw order) against the degree
   distributions written by the reference `-A scm` itself (tests/golden/scm_dd,
   made by tests/golden/make_golden.py) -- byte-for-byte;
-* the model's hand-checkable cases (SURVEY test pyramid item 2): p = 1, p = 0,
+* the model's hand-checkable cases: p = 1, p = 0,
   seed shapes, duplicate retries, id-width boundaries;
-* the oracle's own Philox-mode digests (regression pin).
+* the oracle's own Philox-mode digests (regression pin);
+* the repeated-nodes BA model (-A sba): MT_REF mode against the reference
+  `-A sba` degree distributions, and a literal replay on the endpoint array.
 """
 import json
 import os
@@ -218,3 +220,99 @@ def test_csr_sorted_and_symmetric():
         und = np.concatenate([can, can[:, ::-1]])
         order = np.lexsort((und[:, 1], und[:, 0]))
         assert (und[order, 1] == col).all()
+
+
+# ---- repeated-nodes BA (-A sba) ---------------------------------------------
+
+def _sba_runs():
+    with open(os.path.join(GOLD, "sba_dd.json")) as f:
+        return json.load(f)["runs"]
+
+
+@pytest.mark.parametrize("run", [r for r in _sba_runs() if r["n"] <= 100000],
+                         ids=lambda r: f"n{r['n']}_m{r['m']}")
+def test_ba_mt_ref_mode_reproduces_reference_sba(run):
+    """The oracle's BA model driven by the reference's RNG gives the exact
+    degree distribution the reference -A sba writes."""
+    G = orc.generate_ba(run["n"], run["m"], 5489, orc.RNG_MT_REF)
+    mine = orc.dd_csv_from_degrees(orc.degrees(G, orc.SEED_STAR_REF))
+    with open(os.path.join(GOLD, run["file"])) as f:
+        assert mine == f.read()
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("run", [r for r in _sba_runs() if r["n"] > 100000],
+                         ids=lambda r: f"n{r['n']}_m{r['m']}")
+def test_ba_mt_ref_mode_reproduces_reference_sba_large(run):
+    G = orc.generate_ba(run["n"], run["m"], 5489, orc.RNG_MT_REF)
+    mine = orc.dd_csv_from_degrees(orc.degrees(G, orc.SEED_STAR_REF))
+    with open(os.path.join(GOLD, run["file"])) as f:
+        assert mine == f.read()
+
+
+@pytest.mark.parametrize("case", json.load(open(os.path.join(GOLD, "ba_philox_digests.json")))["cases"],
+                         ids=lambda c: f"n{c['n']}_d{c['d']}_s{c['seed']}")
+def test_ba_philox_digests(case):
+    G, retries = orc.generate_ba(case["n"], case["d"], case["seed"], orc.RNG_PHILOX,
+                                 with_retries=True)
+    slot = orc.pairs_slot_order(G, orc.SEED_STAR_REF)
+    assert slot.shape[0] == case["edges"]
+    assert retries == case["retries"]
+    assert f"{orc.fnv1a64(slot):016x}" == case["fnv_slot_i64"]
+
+
+@pytest.mark.parametrize("d", [1, 2, 5])
+@pytest.mark.parametrize("rng", [orc.RNG_PHILOX, orc.RNG_MT_REF])
+def test_ba_replay_on_endpoint_array(d, rng):
+    """Replay the reference loop literally (src/PA/SPA/SerialBA.cpp:93-161):
+    keep the endpoint array -- node i < d repeated 2d times, then per node w
+    its pairs (target, w) -- and index it with each draw.  The oracle's closed
+    form decode must pick the same endpoints."""
+    n, seed = 400, 2024
+    G, retries = orc.generate_ba(n, d, seed, rng, with_retries=True)
+    mt = orc.mt19937_64(seed, 200000) if rng == orc.RNG_MT_REF else None
+    mt_pos = 0
+    ends = [i for i in range(d) for _ in range(2 * d)]
+    targets = list(range(d))          # node d's targets
+    replay_retries = 0
+    for u in range(d, n):
+        for t in targets:
+            ends += [t, u]
+        if u + 1 == n:
+            break
+        Z = len(ends)
+        assert Z == 2 * d * d + 2 * d * (u + 1 - d)
+        targets = []
+        for i in range(d):
+            r = 0
+            while True:
+                if rng == orc.RNG_PHILOX:
+                    v = u + 1
+                    w = orc.philox((v & 0xFFFFFFFF, v >> 32, i, r), (seed & 0xFFFFFFFF, seed >> 32))
+                    R = ((((w[1] << 32) | w[0]) * Z) >> 64)
+                else:
+                    R = int(mt[mt_pos]) % Z
+                    mt_pos += 1
+                cand = ends[R]
+                if cand not in targets:
+                    targets.append(cand)
+                    break
+                r += 1
+                replay_retries += 1
+        assert targets == G[u + 1].tolist()
+    assert replay_retries == retries
+
+
+@pytest.mark.parametrize("d", [1, 3, 8, 32])
+def test_ba_simple_graph_properties(d):
+    n = 3000
+    G = orc.generate_ba(n, d, 500 + d)
+    _check_simple_graph(G, d, orc.SEED_STAR_REF)
+    assert G[d].tolist() == list(range(d))
+
+
+def test_ba_rejects_bad_shapes():
+    with pytest.raises(ValueError):
+        orc.generate_ba(4, 4, 1)
+    with pytest.raises(ValueError):
+        orc.generate_ba(10, 0, 1)

@@ -6,8 +6,10 @@
 //                [--show-dd 1 --dd-filename dd.csv] [-o outdir]
 //                [--out edges.txt --format text|binary] [--csr]
 //
-// -A cuppa and -A cuppa-adaptive both run the one persistent launch; -s is
-// accepted and ignored (there are no stages).  Prints "Computation Time: <s>"
+// -A cuppa and -A cuppa-adaptive both run the copy model (-s is accepted and
+// ignored: there are no stages); -A scm is the same model with the reference's
+// star seed (src/PA/SPA/SerialCopyModel3.cpp); -A sba is the repeated-nodes
+// Barabasi-Albert model (src/PA/SPA/SerialBA.cpp), star seed, -a ignored.  Prints "Computation Time: <s>"
 // like the reference (src/PA/cuPPA/cuPPA_1.cu:511) plus the device counters.
 // Errors are reported with their pa_strerror text and exit status 1.
 #include <cuda_runtime.h>
@@ -25,7 +27,7 @@ namespace {
 void usage()
 {
     std::fprintf(stderr,
-                 "usage: cuppa_runner -A cuppa|cuppa-adaptive -n N -x M -a P [--seed S]\n"
+                 "usage: cuppa_runner -A cuppa|cuppa-adaptive|scm|sba -n N -x M -a P [--seed S]\n"
                  "       [--id-bits 32|64] [--seed-mode clique|star] [-b B] [-t T] [-s S]\n"
                  "       [--show-dd 0|1] [--dd-filename F] [-o DIR] [--out FILE]\n"
                  "       [--format text|binary] [--csr]\n");
@@ -45,7 +47,7 @@ int main(int argc, char **argv)
     pa_params prm;
     pa_params_init(&prm);
     std::string algo = "cuppa", outdir = "./", ddfile = "degreeDistribution.txt", out, format = "text";
-    bool show_dd = false, csr = false;
+    bool show_dd = false, csr = false, seed_given = false;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
         auto val = [&]() -> const char * {
@@ -64,7 +66,10 @@ int main(int argc, char **argv)
         else if (a == "-s" || a == "--stages" || a == "-w" || a == "--warps") (void)val();
         else if (a == "--seed") prm.seed = std::strtoull(val(), nullptr, 10);
         else if (a == "--id-bits") prm.id_bits = (uint32_t)std::strtoul(val(), nullptr, 10);
-        else if (a == "--seed-mode") prm.seed_mode = std::string(val()) == "star" ? PA_SEED_STAR_REF : PA_SEED_CLIQUE;
+        else if (a == "--seed-mode") {
+            prm.seed_mode = std::string(val()) == "star" ? PA_SEED_STAR_REF : PA_SEED_CLIQUE;
+            seed_given = true;
+        }
         else if (a == "--show-dd") show_dd = std::atoi(val()) != 0;
         else if (a == "--dd-filename") ddfile = val();
         else if (a == "-o" || a == "--output") outdir = val();
@@ -74,8 +79,11 @@ int main(int argc, char **argv)
         else if (a == "-h" || a == "--help") { usage(); return 0; }
         else { usage(); return 2; }
     }
-    if (algo != "cuppa" && algo != "cuppa-adaptive") {
-        std::fprintf(stderr, "only -A cuppa / cuppa-adaptive are provided here\n");
+    if (algo == "scm" || algo == "sba") {
+        if (!seed_given) prm.seed_mode = PA_SEED_STAR_REF;
+        if (algo == "sba") prm.model = PA_MODEL_BA;
+    } else if (algo != "cuppa" && algo != "cuppa-adaptive") {
+        std::fprintf(stderr, "only -A cuppa / cuppa-adaptive / scm / sba are provided here\n");
         return 2;
     }
     if (prm.threads != 0 && prm.threads != 256) prm.threads = 0;   // advisory, as -b

@@ -54,6 +54,7 @@ int make_plan(const pa_params *prm, GenPlan *plan)
     p.seed_edges = pa_seed_edge_count(prm->d, prm->seed_mode);
     p.n_edges = p.seed_edges + n_gen * prm->d;
     p.pth = p_threshold(prm->p);
+    p.model = prm->model;
     p.edges_bytes = p.n_edges * 2ull * p.id_bytes;
     p.n_sb = (p.n_tiles + kSbTiles - 1) / kSbTiles;
     p.sb_offset = kCtlBytes + ((p.n_tiles * 4ull + 255ull) & ~255ull);
@@ -129,7 +130,9 @@ int pa_params_check(const pa_params *prm)
         return PA_ERR_INVALID;
     if (prm->threads != 0 && prm->threads != 256) return PA_ERR_NOT_SUPPORTED;
     if ((prm->flags & ~PA_FLAG_TEST_WITHHOLD_FIRST_TILE) != 0) return PA_ERR_INVALID;
-    if (prm->claim_tiles > 64 || prm->reserved0 != 0) return PA_ERR_INVALID;
+    if (prm->claim_tiles > 64) return PA_ERR_INVALID;
+    if (prm->model != PA_MODEL_COPY && prm->model != PA_MODEL_BA) return PA_ERR_INVALID;
+    if (prm->model == PA_MODEL_BA && prm->seed_mode != PA_SEED_STAR_REF) return PA_ERR_INVALID;
     return PA_OK;
 }
 

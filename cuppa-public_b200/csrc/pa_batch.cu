@@ -320,6 +320,7 @@ int batch_bind(BatchJob &J, const pa_params *prms, void *const *d_edges, const u
         a.min_window = 0;
         a.start_end = p.u_split;
         a.claim_tiles = J.claim_tiles;
+        a.model = p.model;
 
         std::memcpy(table + i, &a, sizeof(a));
         if (i == 0) J.first = a;

@@ -55,6 +55,22 @@ __device__ __forceinline__ Draw draw_slot(uint64_t u, uint32_t i, uint32_t r, ui
     return out;
 }
 
+// One draw of the BA model (endpoint R = floor(x * 2du / 2^64), split as
+// v = floor(x*u / 2^64), q = floor(2d * (x*u mod 2^64) / 2^64)):
+//   direct = q odd, k = q / 2.
+__device__ __forceinline__ Draw draw_slot_ba(uint64_t u, uint32_t i, uint32_t r, uint32_t key0,
+                                             uint32_t key1, uint32_t d)
+{
+    const uint4 w = philox4x32_10(make_uint4((uint32_t)u, (uint32_t)(u >> 32), i, r), key0, key1);
+    const uint64_t x = ((uint64_t)w.y << 32) | w.x;
+    const uint32_t q = (uint32_t)__umul64hi(x * u, 2ull * d);
+    Draw out;
+    out.v = __umul64hi(x, u);
+    out.k = q >> 1;
+    out.direct = q & 1u;
+    return out;
+}
+
 // Slot k of seed node v (v <= d): STAR_REF (0) or CLIQUE (1).
 __device__ __forceinline__ uint64_t seed_slot(uint64_t v, uint32_t k, uint32_t d, uint32_t mode)
 {

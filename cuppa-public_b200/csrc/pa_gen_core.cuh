@@ -48,6 +48,7 @@ struct GenArgs {
     uint64_t min_window;       //   to reach tb - max(min_window, tb >> window_shift)
     uint64_t start_end;        // start kernel: nodes [u_first, start_end) are its work
     uint32_t claim_tiles;      // tiles per claim-counter atomic
+    uint32_t model;            // PA_MODEL_COPY or PA_MODEL_BA
 };
 
 // Record a device-side error once, in the control block and every replica.
@@ -81,6 +82,15 @@ __device__ __forceinline__ void seed_edge(uint64_t e, uint32_t d, uint32_t mode,
 // One draw in node arithmetic of width NodeT (see draw_slot in pa_device.cuh;
 // identical values: for u < 2^32, floor(x*u / 2^64) with x = w1:w0 equals
 // floor((w1*u + floor(w0*u / 2^32)) / 2^32)).
+//
+// BA model (src/PA/SPA/SerialBA.cpp:145-157): the endpoint index is R =
+// floor(x * 2du / 2^64), uniform over the 2du endpoints before node u.  With
+// x*u = v*2^64 + f, R = 2d*v + floor(2d*f / 2^64), so v = floor(x*u / 2^64) is
+// the node of the endpoint pair (v < d: a seed block entry, which is v itself),
+// q = floor(2d*f / 2^64) < 2d its position: odd -> v, even -> v's slot q/2.
+// Seed slots of STAR_REF already map v < d to v and node d to slot k, so the
+// draw becomes (v, k = q/2, direct = q odd) and the rest of the kernel is the
+// copy model's.
 template <typename NodeT>
 struct DrawT {
     NodeT v;
@@ -97,10 +107,18 @@ __device__ __forceinline__ DrawT<NodeT> draw(NodeT u, uint32_t i, uint32_t r, co
         const uint64_t lo = (uint64_t)w.x * u;
         const uint64_t hi = (uint64_t)w.y * u + (lo >> 32);
         out.v = (uint32_t)(hi >> 32);
-        out.k = __umulhi(w.w, a.d);
-        out.direct = (uint64_t)w.z < a.pth;
+        if (a.model == PA_MODEL_BA) {
+            const uint64_t f = (hi << 32) | (uint32_t)lo;   // x*u mod 2^64
+            const uint32_t q = (uint32_t)__umul64hi(f, 2ull * a.d);
+            out.k = q >> 1;
+            out.direct = q & 1u;
+        } else {
+            out.k = __umulhi(w.w, a.d);
+            out.direct = (uint64_t)w.z < a.pth;
+        }
     } else {
-        const Draw dr = draw_slot(u, i, r, a.key0, a.key1, a.pth, a.d);
+        const Draw dr = a.model == PA_MODEL_BA ? draw_slot_ba(u, i, r, a.key0, a.key1, a.d)
+                                               : draw_slot(u, i, r, a.key0, a.key1, a.pth, a.d);
         out.v = dr.v;
         out.k = dr.k;
         out.direct = dr.direct;

@@ -406,6 +406,7 @@ int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, vo
 
     a.start_end = plan.u_split;
     a.claim_tiles = plan.claim_tiles;
+    a.model = plan.model;
 
 
     const uint32_t blocks = blocks_override ? blocks_override : prm->blocks;

@@ -42,6 +42,8 @@ PA_ERR_NOT_FOUND = 8
 
 PA_SEED_STAR_REF = 0
 PA_SEED_CLIQUE = 1
+PA_MODEL_COPY = 0   # copy model (-A cuppa, -A scm)
+PA_MODEL_BA = 1     # repeated-nodes Barabasi-Albert (-A sba); STAR_REF seed only
 PA_LAYOUT_PAIRS = 0
 PA_FORMAT_TEXT = 0
 PA_FORMAT_BINARY = 1
@@ -78,7 +80,7 @@ class PaParams(ctypes.Structure):
         ("spin_limit_ns", ctypes.c_uint64),
         ("start_nodes", ctypes.c_uint64),
         ("claim_tiles", ctypes.c_uint32),
-        ("reserved0", ctypes.c_uint32),
+        ("model", ctypes.c_uint32),
     ]
 
 
@@ -246,14 +248,15 @@ def check(status: int, where: str) -> None:
 def make_params(n: int, d: int, p: float, seed: int = 42, id_bits: int = 32,
                 seed_mode: int = PA_SEED_CLIQUE, blocks: int = 0, threads: int = 0,
                 tile_passes: int = 0, flags: int = 0, spin_limit_ns: int = 0,
-                start_nodes: int = 0, claim_tiles: int = 0) -> PaParams:
+                start_nodes: int = 0, claim_tiles: int = 0,
+                model: int = 0) -> PaParams:
     prm = PaParams()
     check(lib().pa_params_init(ctypes.byref(prm)), "pa_params_init")
     prm.n, prm.d, prm.p, prm.seed = n, d, float(p), seed
     prm.id_bits, prm.seed_mode = id_bits, seed_mode
     prm.blocks, prm.threads, prm.tile_passes = blocks, threads, tile_passes
     prm.flags, prm.spin_limit_ns, prm.start_nodes = flags, spin_limit_ns, start_nodes
-    prm.claim_tiles = claim_tiles
+    prm.claim_tiles, prm.model = claim_tiles, model
     return prm
 
 
@@ -499,6 +502,39 @@ class cuPPA:  # noqa: N801 - reference class name
     def printDegreeDistribution(self, conf: ExperimentConfiguration) -> str:
         """cuPPA.cu:103-165 -- degrees on the device, 'Degree,Count' CSV to
         outputDir/distfile1."""
+        if self.edges is None:
+            raise RuntimeError("generateGraph first")
+        path = os.path.join(conf._outputDir, conf._distfile1)
+        write_degree_distribution(self._prm, self.edges, path)
+        with open(path) as f:
+            return f.read()
+
+
+class SerialBA:  # noqa: N801 - reference class name
+    """SerialBA(nNodes, mEdgesPerNode) -- src/PA/SPA/SerialBA.h:17-37, the
+    repeated-nodes Barabasi-Albert generator of -A sba, run on the device
+    (model PA_MODEL_BA, the reference's star seed).  generateGraph keeps the
+    edges (``self.edges``: node M's edges to 0..M-1, then each later node's M
+    edges in draw order); printDegreeDistribution writes the "Degree,Count" CSV
+    of src/PA/SPA/PAHelper.hpp:69-147."""
+
+    def __init__(self, nNodes: int, mEdgesPerNode: int):
+        self._N, self._M = int(nNodes), int(mEdgesPerNode)
+        self.edges = None
+        self.stats: Optional[PaStats] = None
+        self._prm: Optional[PaParams] = None
+
+    def generateGraph(self, conf: ExperimentConfiguration):
+        self._N, self._M = int(conf._n1), int(conf._x1)
+        self._prm = make_params(self._N, self._M, 0.0, seed=conf.seed, id_bits=conf.id_bits,
+                                seed_mode=PA_SEED_STAR_REF, blocks=conf._blockSize,
+                                model=PA_MODEL_BA)
+        self.edges, self.stats = generate(self._prm)
+        if conf._FLAG_SHOW_DEGREE_DISTRIBUTION:
+            self.printDegreeDistribution(conf)
+        return self.edges
+
+    def printDegreeDistribution(self, conf: ExperimentConfiguration) -> str:
         if self.edges is None:
             raise RuntimeError("generateGraph first")
         path = os.path.join(conf._outputDir, conf._distfile1)

@@ -80,8 +80,23 @@ typedef struct pa_params {
                                persistent launch, at most 2^31.  0 = auto (as many as
                                that allows), PA_START_NONE = none                        */
     uint32_t claim_tiles;   /* tiles claimed per work-counter atomic (1..64); 0 = auto   */
-    uint32_t reserved0;     /* must be 0                                                  */
+    uint32_t model;         /* PA_MODEL_*: the attachment rule                            */
 } pa_params;
+
+/* pa_params.model.
+ * PA_MODEL_COPY -- the copy model of -A cuppa / -A scm: each slot links to a
+ *   uniform earlier node with probability p, else copies a uniform slot of it.
+ * PA_MODEL_BA -- the repeated-nodes Barabasi-Albert model of -A sba
+ *   (src/PA/SPA/SerialBA.cpp:68-186): each slot picks a uniform endpoint of all
+ *   earlier edges, i.e. a node with probability proportional to its degree.
+ *   Requires seed_mode PA_SEED_STAR_REF (the reference's initial graph); p is
+ *   ignored.  The draw of slot i of node u at retry r: x = w1:w0 of
+ *   Philox(ctr = (u_lo, u_hi, i, r)), R = floor(x * 2du / 2^64) indexes the
+ *   endpoint list (2d^2 seed entries, then (target_j, w) per earlier node w),
+ *   so v = floor(x * u / 2^64), q = R mod 2d: q odd -> v itself, q even ->
+ *   v's slot q/2.  Same output layout, duplicate retries and slot order. */
+#define PA_MODEL_COPY 0u
+#define PA_MODEL_BA 1u
 
 /* pa_params.start_nodes: no start kernel (the persistent launch does every node). */
 #define PA_START_NONE UINT64_MAX

@@ -109,10 +109,15 @@ def test_start_split(pa):
     assert split(100, 4, 10 ** 9) == 100
 
 
-def test_claim_tiles_and_reserved_checked(pa):
+def test_claim_tiles_and_model_checked(pa):
     prm = pa.make_params(1000, 4, 0.5, claim_tiles=65)
     assert pa.lib().pa_params_check(ctypes.byref(prm)) == pa.PA_ERR_INVALID
     prm = pa.make_params(1000, 4, 0.5, claim_tiles=64)
     assert pa.lib().pa_params_check(ctypes.byref(prm)) == pa.PA_OK
-    prm.reserved0 = 1
+    prm.model = 2
     assert pa.lib().pa_params_check(ctypes.byref(prm)) == pa.PA_ERR_INVALID
+    # BA runs on the reference's star seed only
+    prm = pa.make_params(1000, 4, 0.5, model=pa.PA_MODEL_BA, seed_mode=pa.PA_SEED_CLIQUE)
+    assert pa.lib().pa_params_check(ctypes.byref(prm)) == pa.PA_ERR_INVALID
+    prm = pa.make_params(1000, 4, 0.5, model=pa.PA_MODEL_BA, seed_mode=pa.PA_SEED_STAR_REF)
+    assert pa.lib().pa_params_check(ctypes.byref(prm)) == pa.PA_OK

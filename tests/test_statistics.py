@@ -64,6 +64,17 @@ def test_oracle_matches_reference_distribution(p):
     assert abs(tail_alpha(mine) - tail_alpha(ref)) < ALPHA_TOL
 
 
+def test_ba_oracle_matches_reference_sba_distribution():
+    """The BA model with Philox draws against the reference -A sba run
+    (tests/golden/sba_dd, MT19937-64) at n = 10^6, M = 4."""
+    G = orc.generate_ba(10 ** 6, 4, 1)
+    mine = _hist(orc.dd_csv_from_degrees(orc.degrees(G, orc.SEED_STAR_REF)))
+    with open(os.path.join(GOLD, "sba_dd", "sba_n1000000_m4.csv")) as f:
+        ref = _hist(f.read())
+    assert ks_statistic(mine, ref) < KS_BOUND
+    assert abs(tail_alpha(mine) - tail_alpha(ref)) < ALPHA_TOL
+
+
 def test_p0_degenerate_matches_reference_exactly():
     with open(os.path.join(GOLD, "scm_dd", "scm_n10000_m4_p0.0.csv")) as f:
         ref = f.read()

@@ -47,6 +47,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "cuppa-public_b200"))
 
 CLIQUE, STAR_REF = 1, 0
+COPY, BA = 0, 1
 WORKLOADS = {
     "c3": dict(n=2 ** 30, d=4, p=0.5, seed=1234, id_bits=64, seed_mode=CLIQUE,
                name="copy-model PA, n=2^30, d=4, p=0.5, int64 ids, clique seed, Philox seed 1234"),
@@ -62,6 +63,11 @@ WORKLOADS = {
                      "(traffic capture size)"),
     "c1": dict(n=10 ** 5, d=4, p=0.5, seed=42, id_bits=32, seed_mode=CLIQUE,
                name="copy-model PA, n=10^5, d=4, p=0.5, int32 ids, clique seed, Philox seed 42"),
+    # the repeated-nodes Barabasi-Albert model of -A sba at the same size
+    "sba": dict(n=2 ** 30, d=4, p=0.0, seed=1234, id_bits=64, seed_mode=STAR_REF, model=BA,
+                name="repeated-nodes BA (-A sba), n=2^30, d=4, int64 ids, star seed, "
+                     "Philox seed 1234",
+                metric="edges/s on 1 B200 (BA PA generation)"),
 }
 METRIC = "edges/s on 1 B200 (copy-model PA generation)"
 CPU_SAMPLE_NODES = 2 ** 24      # oracle sample: ~67M edges, a few seconds on one core
@@ -69,9 +75,11 @@ REF_SAMPLE_NODES = 2 ** 23      # reference scm sample per step: ~33.5M edges
 
 
 def algorithmic_bytes_per_edge(w) -> float:
-    """2s (pair write) + (1-p)s (copy-target read), s = id bytes."""
+    """2s (pair write) + c*s (copy-target read), s = id bytes; c = 1-p for the
+    copy model, 1/2 for BA (an even endpoint position is a target slot)."""
     s = w["id_bits"] // 8
-    return 2 * s + (1.0 - w["p"]) * s
+    copy = 0.5 if w.get("model", COPY) == BA else 1.0 - w["p"]
+    return 2 * s + copy * s
 
 
 def load_peaks():
@@ -180,11 +188,16 @@ def cpu_baseline_oracle(w, nodes: int):
     import _oracle as orc
     n = min(nodes, w["n"])
     t0 = time.perf_counter()
-    orc.generate(n, w["d"], w["p"], w["seed"], w["seed_mode"])
+    if w.get("model", COPY) == BA:
+        orc.generate_ba(n, w["d"], w["seed"])
+        what = "Philox restatement of SerialBA.cpp"
+    else:
+        orc.generate(n, w["d"], w["p"], w["seed"], w["seed_mode"])
+        what = "Philox restatement of SerialCopyModel3.cpp"
     dt = time.perf_counter() - t0
     edges = orc.edge_count(n, w["d"], w["seed_mode"])
     return {"value": edges / dt, "unit": "edges/s", "cores": 1, "kind": "port",
-            "sample": f"oracle (Philox restatement of SerialCopyModel3.cpp), n={n}, d={w['d']}, "
+            "sample": f"oracle ({what}), n={n}, d={w['d']}, "
                       f"p={w['p']}, {edges} edges in {dt:.2f} s, one thread"}
 
 
@@ -192,18 +205,26 @@ def run_reference(args, w):
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    ref = os.path.join(ROOT, "oracle", "_ref", "scm_ref")
+    ba = w.get("model", COPY) == BA
+    ref = os.path.join(ROOT, "oracle", "_ref", "sba_ref" if ba else "scm_ref")
     n = REF_SAMPLE_NODES
     d = w["d"]
     edges = (n - d - 1) * d + d
     times = []
     if os.path.exists(ref):
         kind = "reference"
-        sample = (f"reference -A scm (SerialCopyModel3.cpp, MT19937-64, star seed, int32 ids), "
-                  f"n={n}, d={d}, p={w['p']}; its own 'Computation Time' per step; single-threaded")
+        if ba:
+            sample = (f"reference -A sba (SerialBA.cpp, MT19937-64, int32 ids), n={n}, d={d}; "
+                      "its own 'Computation Time' per step; single-threaded")
+            cmd = [ref, str(n), str(d), "{td}", "-"]
+        else:
+            sample = (f"reference -A scm (SerialCopyModel3.cpp, MT19937-64, star seed, int32 ids), "
+                      f"n={n}, d={d}, p={w['p']}; its own 'Computation Time' per step; "
+                      "single-threaded")
+            cmd = [ref, str(n), str(d), str(w["p"]), "{td}", "-"]
         with tempfile.TemporaryDirectory() as td:
             for i in range(args.warmup + args.steps):
-                out = subprocess.run([ref, str(n), str(d), str(w["p"]), td, "-"], cwd=td,
+                out = subprocess.run([td if a == "{td}" else a for a in cmd], cwd=td,
                                      capture_output=True, text=True, check=True).stdout
                 t = [float(x.split(":")[1]) for x in out.splitlines()
                      if x.startswith("Computation Time")][0]
@@ -217,13 +238,16 @@ def run_reference(args, w):
         edges = orc.edge_count(n, d, w["seed_mode"])
         for i in range(args.warmup + args.steps):
             t0 = time.perf_counter()
-            orc.generate(n, d, w["p"], w["seed"], w["seed_mode"])
+            if ba:
+                orc.generate_ba(n, d, w["seed"])
+            else:
+                orc.generate(n, d, w["p"], w["seed"], w["seed_mode"])
             if i >= args.warmup:
                 times.append(time.perf_counter() - t0)
     total = sum(times)
     value = edges * len(times) / total
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "edges/s",
+        "impl": "reference", "metric": w.get("metric", METRIC), "value": value, "unit": "edges/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * total / len(times), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int64" if w["id_bits"] == 64 else "int32",
@@ -251,7 +275,7 @@ def run_gpu(args, w):
 
     prm = pa.make_params(w["n"], w["d"], w["p"], seed=w["seed"], id_bits=w["id_bits"],
                          seed_mode=w["seed_mode"], tile_passes=args.tile_passes,
-                         blocks=args.blocks)
+                         blocks=args.blocks, model=w.get("model", COPY))
     E = pa.edge_count(prm)
     edges, scratch = pa.alloc_buffers(prm)
     stream = torch.cuda.Stream()
@@ -339,7 +363,7 @@ def run_gpu(args, w):
         achieved = k_edges * bpe / kern_s / 1e9
         launches = (1 if u_split > w["d"] + 1 else 0) + (1 if gen_edges > 0 else 0)
         line = {
-            "metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": world,
+            "metric": w.get("metric", METRIC), "value": value, "unit": "edges/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "int64" if w["id_bits"] == 64 else "int32",

@@ -55,7 +55,8 @@ int make_plan(const pa_params *prm, GenPlan *plan)
     p.n_edges = p.seed_edges + n_gen * prm->d;
     p.pth = p_threshold(prm->p);
     p.model = prm->model;
-    p.edges_bytes = p.n_edges * 2ull * p.id_bytes;
+    p.slots = prm->layout == PA_LAYOUT_SLOTS;
+    p.edges_bytes = p.slots ? n_gen * prm->d * p.id_bytes : p.n_edges * 2ull * p.id_bytes;
     p.n_sb = (p.n_tiles + kSbTiles - 1) / kSbTiles;
     p.sb_offset = kCtlBytes + ((p.n_tiles * 4ull + 255ull) & ~255ull);
     p.trace_offset = p.sb_offset + ((p.n_sb * 4ull + 255ull) & ~255ull);
@@ -95,6 +96,7 @@ const char *pa_strerror(int status)
     case PA_ERR_NOT_SUPPORTED: return "not supported";
     case PA_ERR_BUSY: return "busy: admission refused";
     case PA_ERR_NOT_FOUND: return "unknown ticket";
+    case PA_ERR_IO: return "file or sink error";
     default: return "unknown status";
     }
 }
@@ -124,7 +126,10 @@ int pa_params_check(const pa_params *prm)
     if (prm->n > (1ull << 40)) return PA_ERR_INVALID;
     if (!(prm->p >= 0.0 && prm->p <= 1.0)) return PA_ERR_INVALID;
     if (prm->seed_mode != PA_SEED_STAR_REF && prm->seed_mode != PA_SEED_CLIQUE) return PA_ERR_INVALID;
-    if (prm->layout != PA_LAYOUT_PAIRS) return PA_ERR_NOT_SUPPORTED;
+    if (prm->layout != PA_LAYOUT_PAIRS && prm->layout != PA_LAYOUT_SLOTS) return PA_ERR_NOT_SUPPORTED;
+    if (prm->layout == PA_LAYOUT_SLOTS &&
+        (prm->start_nodes != 0 || prm->n - prm->d - 1 > kStartNodesAuto))
+        return PA_ERR_NOT_SUPPORTED;
     if (prm->tile_passes != 0 && prm->tile_passes != 1 && prm->tile_passes != 2 &&
         prm->tile_passes != 4 && prm->tile_passes != 8)
         return PA_ERR_INVALID;

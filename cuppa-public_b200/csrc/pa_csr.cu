@@ -572,7 +572,7 @@ int csr_enqueue(const pa_params *prm, const void *d_edges, int64_t *d_rowptr, vo
     const int rc = make_plan(prm, &p);
     if (rc != PA_OK) return rc;
     if (!d_edges || !d_rowptr || !d_col || !d_scratch) return PA_ERR_INVALID;
-    if (!csr_supported(prm->n)) return PA_ERR_NOT_SUPPORTED;
+    if (!csr_supported(prm->n) || p.slots) return PA_ERR_NOT_SUPPORTED;
     if ((reinterpret_cast<uintptr_t>(d_col) & 15u) || (reinterpret_cast<uintptr_t>(d_scratch) & 15u))
         return PA_ERR_INVALID;
     const CsrLayout L = csr_layout(prm->n, prm->d, p.n_edges);
@@ -598,7 +598,7 @@ int pa_csr_bytes(const pa_params *prm, uint64_t *rowptr_bytes, uint64_t *col_byt
     const int rc = make_plan(prm, &p);
     if (rc != PA_OK) return rc;
     if (!rowptr_bytes || !col_bytes || !scratch_bytes) return PA_ERR_INVALID;
-    if (!csr_supported(prm->n)) return PA_ERR_NOT_SUPPORTED;
+    if (!csr_supported(prm->n) || p.slots) return PA_ERR_NOT_SUPPORTED;
     *rowptr_bytes = 8 * (prm->n + 1);
     *col_bytes = 2 * p.n_edges * p.id_bytes;
     *scratch_bytes = csr_layout(prm->n, prm->d, p.n_edges).total;

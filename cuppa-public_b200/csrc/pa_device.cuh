@@ -71,6 +71,22 @@ __device__ __forceinline__ Draw draw_slot_ba(uint64_t u, uint32_t i, uint32_t r,
     return out;
 }
 
+// e-th canonical seed edge (e < seed edge count): CLIQUE (1) rows v = 1..d hold
+// (v, 0..v-1); STAR_REF (0) is node d -> 0..d-1.
+__device__ __forceinline__ void seed_edge_of(uint64_t e, uint32_t d, uint32_t mode, uint64_t &src,
+                                             uint64_t &dst)
+{
+    if (mode == 1) {
+        uint64_t v = 1, base = 0;
+        while (base + v <= e) { base += v; ++v; }
+        src = v;
+        dst = e - base;
+    } else {
+        src = d;
+        dst = e;
+    }
+}
+
 // Slot k of seed node v (v <= d): STAR_REF (0) or CLIQUE (1).
 __device__ __forceinline__ uint64_t seed_slot(uint64_t v, uint32_t k, uint32_t d, uint32_t mode)
 {
@@ -222,6 +238,17 @@ __device__ __forceinline__ void st_relaxed_pair(int32_t *p, uint64_t a, uint64_t
     asm volatile("st.relaxed.gpu.global.v2.u32 [%0], {%1, %2};" ::"l"(p), "r"((uint32_t)a),
                  "r"((uint32_t)b)
                  : "memory");
+}
+
+// gpu-scope relaxed store of one id (the SLOTS layout's counterpart).
+__device__ __forceinline__ void st_relaxed_id(int64_t *p, uint64_t v)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ void st_relaxed_id(int32_t *p, uint64_t v)
+{
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"((uint32_t)v) : "memory");
 }
 
 __device__ __forceinline__ void st_pair2(int32_t *p, uint64_t a, uint64_t b, uint64_t c, uint64_t d)

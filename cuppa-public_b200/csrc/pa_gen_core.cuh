@@ -30,7 +30,8 @@ struct GenArgs {
     uint64_t u_first;
     uint64_t n_tiles;
     uint64_t seed_edges;
-    int64_t slot_off;     // pair index of slot (v, k) = v*d + k + slot_off, for v > d
+    int64_t slot_off;     // index of slot (v, k) = v*d + k + slot_off, for v > d (a pair
+                          // index in PAIRS; the id index in SLOTS, where seed_edges = 0)
     uint64_t pth;
     uint64_t spin_limit_ns;
     uint32_t key0, key1;
@@ -64,19 +65,11 @@ __device__ __forceinline__ const GenRep *my_rep(const GenArgs &a)
     return a.reps + ((blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)) % kReps);
 }
 
-// e-th canonical seed edge.
+// e-th canonical seed edge (seed_edge_of in pa_device.cuh).
 __device__ __forceinline__ void seed_edge(uint64_t e, uint32_t d, uint32_t mode, uint64_t &src,
                                           uint64_t &dst)
 {
-    if (mode == 1) {  // clique: rows v = 1..d hold (v, 0..v-1)
-        uint64_t v = 1, base = 0;
-        while (base + v <= e) { base += v; ++v; }
-        src = v;
-        dst = e - base;
-    } else {          // star node d -> 0..d-1
-        src = d;
-        dst = e;
-    }
+    seed_edge_of(e, d, mode, src, dst);
 }
 
 // One draw in node arithmetic of width NodeT (see draw_slot in pa_device.cuh;
@@ -137,11 +130,13 @@ __device__ __forceinline__ uint32_t meta_st(uint32_t m) { return m & 3u; }
 __device__ __forceinline__ uint32_t meta_k(uint32_t m) { return (m >> 2) & 63u; }
 __device__ __forceinline__ uint32_t meta_r(uint32_t m) { return m >> 8; }
 
-template <typename Id, typename NodeT>
+// Address of the target of slot (v, k): the second field of its pair (PAIRS)
+// or the id itself (SLOTS).
+template <typename Id, typename NodeT, bool Slots = false>
 __device__ __forceinline__ const Id *slot_addr(const Id *E, const GenArgs &a, NodeT v, uint32_t k)
 {
     const int64_t idx = (int64_t)((uint64_t)v * a.d) + (int64_t)k + a.slot_off;
-    return E + 2 * idx + 1;
+    return Slots ? E + idx : E + 2 * idx + 1;
 }
 
 // Whether the superblock holding node v has all its tiles published (the
@@ -455,7 +450,8 @@ struct StartArgs {
 
 // Launch the start kernel; `blocks` 0 = one wave.  The claim counters must be
 // zero and every pair of the graphs' start regions all-ones (fill_start).
-int launch_start(uint32_t id_bytes, const StartArgs &b, uint32_t blocks, cudaStream_t s);
+int launch_start(uint32_t id_bytes, const StartArgs &b, uint32_t blocks, cudaStream_t s,
+                 bool slots = false);
 
 // Set every byte of the pairs of nodes [u_first, start_end) of each of `count`
 // graphs to 0xff (one launch).

@@ -384,8 +384,9 @@ int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, vo
     a.n = prm->n;
     a.u_first = plan.u_first;
     a.n_tiles = plan.n_tiles;
-    a.seed_edges = plan.seed_edges;
-    a.slot_off = (int64_t)plan.seed_edges - (int64_t)(plan.u_first * prm->d);
+    // SLOTS stores no seed rows: its ids start with node u_first's
+    a.seed_edges = plan.slots ? 0 : plan.seed_edges;
+    a.slot_off = (int64_t)a.seed_edges - (int64_t)(plan.u_first * prm->d);
     a.pth = plan.pth;
     a.spin_limit_ns = plan.spin_limit_ns;
     a.key0 = (uint32_t)prm->seed;
@@ -415,10 +416,11 @@ int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, vo
     const bool small = prm->n + plan.tile_nodes + 32 < (1ull << 32);
     if (plan.u_split > plan.u_first) {
         // The start region, with slot-granular waits (pa_start.cu): its pairs
-        // start as all-ones; the start kernel writes them and the seed edges.
-        const uint64_t pair_bytes = 2ull * plan.id_bytes;
-        e = cudaMemsetAsync(reinterpret_cast<unsigned char *>(d_edges) + plan.seed_edges * pair_bytes,
-                            0xff, (plan.u_split - plan.u_first) * prm->d * pair_bytes, stream);
+        // (ids, in SLOTS) start as all-ones; the start kernel writes them and
+        // the seed edges.
+        const uint64_t slot_bytes = (plan.slots ? 1ull : 2ull) * plan.id_bytes;
+        e = cudaMemsetAsync(reinterpret_cast<unsigned char *>(d_edges) + a.seed_edges * slot_bytes,
+                            0xff, (plan.u_split - plan.u_first) * prm->d * slot_bytes, stream);
         if (e != cudaSuccess) return set_cuda_error(e);
         StartArgs sa;
         std::memset(&sa, 0, sizeof(sa));
@@ -431,7 +433,7 @@ int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, vo
         sa.ctl = a.ctl;
         mrc = mark(1);
         if (mrc != PA_OK) return mrc;
-        const int rc = launch_start(plan.id_bytes, sa, blocks, stream);
+        const int rc = launch_start(plan.id_bytes, sa, blocks, stream, plan.slots);
         if (rc != PA_OK) return rc;
         if (plan.u_split >= prm->n) {
             mrc = mark(2);
@@ -440,6 +442,12 @@ int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, vo
         // u_split - u_first is a whole number of superblocks
         a.tile_begin = (plan.u_split - plan.u_first) / plan.tile_nodes;
         a.water_init = a.tile_begin / kSbTiles;
+    }
+    if (plan.slots && plan.u_split <= plan.u_first) {
+        // a seed-only graph stores nothing in SLOTS
+        for (int i = 1; i < 4; ++i)
+            if ((mrc = mark(i)) != PA_OK) return mrc;
+        return PA_OK;
     }
     if (plan.u_split <= plan.u_first) {
         mrc = mark(1);

@@ -66,6 +66,7 @@ struct GenPlan {
     uint64_t n_edges;
     uint64_t pth;           // direct threshold
     uint32_t model;         // PA_MODEL_*
+    bool slots;             // PA_LAYOUT_SLOTS: targets only, seed rows implied
     uint64_t edges_bytes;
     uint64_t scratch_bytes;
     uint64_t spin_limit_ns;

@@ -1,11 +1,6 @@
 // pa_io.cu -- file outputs of a generated graph.
 //
-//  * pa_write_edges: the edge list as text, one "u v" line per edge -- the format
-//    of PAHelper::writeGraphToDisk (src/PA/SPA/PAHelper.hpp:163-177) -- or as raw
-//    little-endian id pairs.  The device buffer is streamed to the file through
-//    two pinned staging buffers, so copy and formatting overlap.  With the
-//    reference's seed graph (PA_SEED_STAR_REF) the PAIRS order is exactly the
-//    reference's row order: node M's star row, then rows M+1..N-1 in slot order.
+//  (pa_write_edges, the edge-list writer, is in pa_stream.cu.)
 //  * pa_write_degree_distribution: the "Degree,Count" CSV of
 //    cuPPA::printDegreeDistribution (src/PA/cuPPA/cuPPA.cu:103-165), degree-0
 //    nodes omitted as there.  Degrees and their histogram are computed on the
@@ -59,105 +54,12 @@ int grid_for(uint64_t items)
     return (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)sms * 4));
 }
 
-// Decimal digits of v into p (no terminator); returns the end.
-inline char *put_u64(char *p, uint64_t v)
-{
-    char tmp[24];
-    int k = 0;
-    do {
-        tmp[k++] = (char)('0' + v % 10);
-        v /= 10;
-    } while (v);
-    while (k) *p++ = tmp[--k];
-    return p;
-}
-
 }  // namespace
 }  // namespace pa
 
 using namespace pa;
 
 extern "C" {
-
-int pa_write_edges(const pa_params *prm, const void *d_edges, const char *path, int format,
-                   void *stream)
-{
-    GenPlan p;
-    int rc = make_plan(prm, &p);
-    if (rc != PA_OK) return rc;
-    if (!d_edges || !path || (format != PA_FORMAT_TEXT && format != PA_FORMAT_BINARY))
-        return PA_ERR_INVALID;
-    FILE *f = std::fopen(path, "wb");
-    if (!f) return PA_ERR_INVALID;
-    cudaStream_t s = (cudaStream_t)stream;
-    const uint64_t pair_bytes = 2ull * p.id_bytes;
-    const uint64_t chunk_pairs = 1ull << 22;   // 4M pairs per staging buffer
-    void *stage[2] = {nullptr, nullptr};
-    cudaEvent_t done[2] = {nullptr, nullptr};
-    cudaError_t e = cudaSuccess;
-    for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
-        e = cudaMallocHost(&stage[i], chunk_pairs * pair_bytes);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming);
-    }
-    std::vector<char> text;
-    if (format == PA_FORMAT_TEXT) text.resize(chunk_pairs * 42);
-    const uint64_t total = p.n_edges;
-    const uint64_t chunks = (total + chunk_pairs - 1) / chunk_pairs;
-    auto issue = [&](uint64_t c) {
-        const uint64_t first = c * chunk_pairs;
-        const uint64_t cnt = std::min(chunk_pairs, total - first);
-        cudaError_t ee = cudaMemcpyAsync(stage[c & 1],
-                                         (const unsigned char *)d_edges + first * pair_bytes,
-                                         cnt * pair_bytes, cudaMemcpyDeviceToHost, s);
-        if (ee == cudaSuccess) ee = cudaEventRecord(done[c & 1], s);
-        return ee;
-    };
-    if (e == cudaSuccess && chunks) e = issue(0);
-    for (uint64_t c = 0; c < chunks && e == cudaSuccess; ++c) {
-        if (c + 1 < chunks) e = issue(c + 1);
-        if (e == cudaSuccess) e = cudaEventSynchronize(done[c & 1]);
-        if (e != cudaSuccess) break;
-        const uint64_t first = c * chunk_pairs;
-        const uint64_t cnt = std::min(chunk_pairs, total - first);
-        size_t wrote, want;
-        if (format == PA_FORMAT_BINARY) {
-            want = cnt * pair_bytes;
-            wrote = std::fwrite(stage[c & 1], 1, want, f);
-        } else {
-            char *q = text.data();
-            for (uint64_t i = 0; i < cnt; ++i) {
-                uint64_t u, v;
-                if (p.id_bytes == 8) {
-                    const int64_t *pp = (const int64_t *)stage[c & 1] + 2 * i;
-                    u = (uint64_t)pp[0];
-                    v = (uint64_t)pp[1];
-                } else {
-                    const int32_t *pp = (const int32_t *)stage[c & 1] + 2 * i;
-                    u = (uint32_t)pp[0];
-                    v = (uint32_t)pp[1];
-                }
-                q = put_u64(q, u);
-                *q++ = ' ';
-                q = put_u64(q, v);
-                *q++ = '\n';
-            }
-            want = (size_t)(q - text.data());
-            wrote = std::fwrite(text.data(), 1, want, f);
-        }
-        if (wrote != want) {
-            rc = PA_ERR_INVALID;
-            break;
-        }
-    }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    for (int i = 0; i < 2; ++i) {
-        if (done[i]) cudaEventDestroy(done[i]);
-        if (stage[i]) cudaFreeHost(stage[i]);
-    }
-    if (std::fclose(f) != 0 && rc == PA_OK) rc = PA_ERR_INVALID;
-    if (e != cudaSuccess) return set_cuda_error(e);
-    return rc;
-}
 
 int pa_write_degree_distribution(const pa_params *prm, const void *d_edges, const char *path,
                                  void *stream)

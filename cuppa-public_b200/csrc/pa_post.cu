@@ -75,6 +75,39 @@ __global__ void degree_kernel(const Id *E, uint64_t n_edges, uint64_t n, unsigne
     }
 }
 
+// The same over a SLOTS graph: a group of d lanes takes one row (node
+// u_first + row, targets S[row*d ..]); the seed edges come from their closed form.
+template <typename Id>
+__global__ void degree_slots_kernel(const Id *S, uint64_t rows, uint32_t d, uint64_t u_first,
+                                    uint32_t seed_mode, uint64_t seed_edges, uint64_t n,
+                                    unsigned long long *deg)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t G = 32u / d;
+    const uint32_t g = lane / d;
+    const bool used = lane < G * d;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    const uint64_t w0 = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (w0 == 0)
+        for (uint64_t e = lane; e < seed_edges; e += 32) {
+            uint64_t s, t;
+            seed_edge_of(e, d, seed_mode, s, t);
+            atomicAdd(deg + s, 1ull);
+            atomicAdd(deg + t, 1ull);
+        }
+    for (uint64_t r0 = w0 * G; r0 < rows; r0 += warps * G) {
+        const uint64_t row = r0 + g;
+        const bool in = used && row < rows;
+        unsigned long long t = in ? (unsigned long long)S[row * d + (lane - g * d)] : ~0ull;
+        const bool act = in && t < n;       // ids are used as addresses: never trust them
+        if (!act) t = ~0ull - lane;
+        const uint32_t mt = __match_any_sync(kFull, t);
+        if (act && (__ffs(mt) - 1) == (int)lane) atomicAdd(deg + t, (unsigned long long)__popc(mt));
+        // the row's own node: d increments, from its first lane
+        if (in && lane == g * d) atomicAdd(deg + u_first + row, (unsigned long long)d);
+    }
+}
+
 int grid_for(uint64_t work_items, uint32_t threads)
 {
     int dev = 0, sms = 148;
@@ -99,6 +132,7 @@ int pa_canonicalize(const pa_params *prm, const void *d_edges, void *d_out, void
     const int rc = make_plan(prm, &p);
     if (rc != PA_OK) return rc;
     if (!d_edges || !d_out) return PA_ERR_INVALID;
+    if (p.slots) return PA_ERR_NOT_SUPPORTED;
     const uint64_t rows = prm->n - p.u_first;
     const uint32_t threads = 256;
     const int grid = grid_for(rows * prm->d, threads);
@@ -124,7 +158,17 @@ int pa_degrees(const pa_params *prm, const void *d_edges, int64_t *d_deg, void *
     if (e != cudaSuccess) return set_cuda_error(e);
     const uint32_t threads = 256;
     const int grid = grid_for(p.n_edges, threads);
-    if (p.n_edges) {
+    if (p.slots) {
+        const uint64_t rows = prm->n - p.u_first;
+        if (p.id_bytes == 8)
+            degree_slots_kernel<int64_t><<<grid, threads, 0, s>>>(
+                (const int64_t *)d_edges, rows, prm->d, p.u_first, prm->seed_mode, p.seed_edges,
+                prm->n, (unsigned long long *)d_deg);
+        else
+            degree_slots_kernel<int32_t><<<grid, threads, 0, s>>>(
+                (const int32_t *)d_edges, rows, prm->d, p.u_first, prm->seed_mode, p.seed_edges,
+                prm->n, (unsigned long long *)d_deg);
+    } else if (p.n_edges) {
         if (p.id_bytes == 8)
             degree_kernel<int64_t><<<grid, threads, 0, s>>>((const int64_t *)d_edges, p.n_edges,
                                                             prm->n, (unsigned long long *)d_deg);

@@ -50,11 +50,11 @@ struct Sentinel {
 
 // Read slot (v, k) into s: true with its value, or false (s.val = v) while it
 // still holds the fill.
-template <typename Id>
+template <typename Id, bool Slots>
 __device__ __forceinline__ bool read_slot(Slot<uint32_t> &s, const GenArgs &a, const Id *E,
                                           uint32_t v, uint32_t k)
 {
-    const uint64_t x = ld_slot(slot_addr(E, a, v, k));
+    const uint64_t x = ld_slot(slot_addr<Id, uint32_t, Slots>(E, a, v, k));
     if (x != Sentinel<Id>::value) {
         s.val = (uint32_t)x;
         return true;
@@ -65,7 +65,7 @@ __device__ __forceinline__ bool read_slot(Slot<uint32_t> &s, const GenArgs &a, c
 
 // Where the candidate of a fresh draw comes from (32-bit node arithmetic: the
 // start region ends below 2^31).
-template <typename Id>
+template <typename Id, bool Slots>
 __device__ __forceinline__ void classify_start(Slot<uint32_t> &s, const DrawT<uint32_t> &dr,
                                                uint32_t r, const GenArgs &a, const Id *E,
                                                uint32_t pbase, uint32_t &n_pend)
@@ -76,7 +76,7 @@ __device__ __forceinline__ void classify_start(Slot<uint32_t> &s, const DrawT<ui
     } else if (dr.v <= a.d) {
         s.val = (uint32_t)seed_slot(dr.v, dr.k, a.d, a.seed_mode);
     } else if (dr.v < pbase) {
-        if (!read_slot<Id>(s, a, E, dr.v, dr.k)) {
+        if (!read_slot<Id, Slots>(s, a, E, dr.v, dr.k)) {
             st = ST_PEND_GLOBAL;
             ++n_pend;
         }
@@ -92,14 +92,16 @@ __device__ __forceinline__ void classify_start(Slot<uint32_t> &s, const DrawT<ui
 // the source lane by shuffle; sources in an earlier pass of the tile are polled
 // in memory like any other.  Returns false when the warp must stop (wait limit,
 // or another warp failed).
-template <typename Id>
+template <typename Id, bool Slots>
 __device__ __forceinline__ bool resolve_start(Slot<uint32_t> (&s)[kStartPasses], const GenArgs &a,
                                               Id *E, uint32_t tb, bool withhold, const Lane &L,
                                               uint32_t &n_retry, uint32_t &n_wait,
                                               uint32_t &n_pend, uint32_t &n_poll)
 {
     const uint32_t d = a.d, G = a.groups;
-    Id *pair0 = E + 2 * (a.seed_edges + (uint64_t)(tb - (uint32_t)a.u_first) * d + L.lane);
+    // this lane's slot of pass 0: a pair (PAIRS) or an id (SLOTS, seed_edges = 0)
+    const uint64_t e_lane = a.seed_edges + (uint64_t)(tb - (uint32_t)a.u_first) * d + L.lane;
+    Id *pair0 = Slots ? E + e_lane : E + 2 * e_lane;
     uint32_t stored = 0;   // bit j: pass j's slot is stored (or inactive)
 #pragma unroll
     for (int j = 0; j < kStartPasses; ++j)
@@ -116,7 +118,7 @@ __device__ __forceinline__ bool resolve_start(Slot<uint32_t> (&s)[kStartPasses],
             const uint32_t u = pbase + L.g;
             const bool active = L.used && u < a.start_end;
             if (active && meta_st(s[j].meta) == ST_PEND_GLOBAL) {
-                if (read_slot<Id>(s[j], a, E, s[j].val, meta_k(s[j].meta))) {
+                if (read_slot<Id, Slots>(s[j], a, E, s[j].val, meta_k(s[j].meta))) {
                     s[j].meta &= ~3u;
                     changed = true;
                 } else {
@@ -130,7 +132,10 @@ __device__ __forceinline__ bool resolve_start(Slot<uint32_t> (&s)[kStartPasses],
             const uint32_t badm = __ballot_sync(kFull, bad);
             const bool fin = active && (badm & L.gmask & L.le) == 0u;
             if (fin && !((stored >> j) & 1u)) {
-                if (!withhold) st_relaxed_pair(pair0 + 2 * (uint64_t)(j * G * d), u, s[j].val);
+                if (!withhold) {
+                    if constexpr (Slots) st_relaxed_id(pair0 + (uint64_t)(j * G * d), s[j].val);
+                    else st_relaxed_pair(pair0 + 2 * (uint64_t)(j * G * d), u, s[j].val);
+                }
                 stored |= 1u << j;
             }
             const uint32_t finm = __ballot_sync(kFull, fin || !active);
@@ -150,7 +155,8 @@ __device__ __forceinline__ bool resolve_start(Slot<uint32_t> (&s)[kStartPasses],
             // a candidate equal to a final lower slot of the node is rejected
             if (known && !fin && (eq & L.lt & L.gmask & finm) != 0u) {
                 const uint32_t r = meta_r(s[j].meta) + 1u;
-                classify_start<Id>(s[j], draw<uint32_t>(u, L.slot, r, a), r, a, E, pbase, n_pend);
+                classify_start<Id, Slots>(s[j], draw<uint32_t>(u, L.slot, r, a), r, a, E, pbase,
+                                          n_pend);
                 changed = true;
                 ++n_retry;
             }
@@ -190,7 +196,7 @@ __device__ __forceinline__ void set_lane(Lane &L, const GenArgs &a)
     L.gmask = L.used ? (a.d == 32 ? kFull : (((1u << a.d) - 1u) << (L.g * a.d))) : 0u;
 }
 
-template <typename Id>
+template <typename Id, bool Slots>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) start_kernel(const StartArgs b)
 {
     __shared__ GenArgs s_args[kThreads / 32];
@@ -209,8 +215,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) start_kernel(const Start
         cur = 0;
     }
 
-    if (b.write_seeds) {
-        // closed forms; nothing reads them back
+    if (!Slots && b.write_seeds) {
+        // closed forms; nothing reads them back (SLOTS does not store them)
         const uint32_t gw = blockIdx.x * (kThreads / 32) + warp;
         const uint32_t nw = gridDim.x * (kThreads / 32);
         for (uint32_t i = gw; i < b.count; i += nw) {
@@ -264,9 +270,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) start_kernel(const Start
             s[j].val = 0;
             s[j].meta = ST_KNOWN;
             if (L.used && u < a.start_end)
-                classify_start<Id>(s[j], draw<uint32_t>(u, L.slot, 0u, a), 0u, a, E, pbase, n_pend);
+                classify_start<Id, Slots>(s[j], draw<uint32_t>(u, L.slot, 0u, a), 0u, a, E, pbase,
+                                          n_pend);
         }
-        ok = resolve_start<Id>(s, a, E, tb, a.withhold_first && t == 0, L, n_retry, n_wait, n_pend,
+        ok = resolve_start<Id, Slots>(s, a, E, tb, a.withhold_first && t == 0, L, n_retry, n_wait, n_pend,
                                n_poll);
     }
 
@@ -314,10 +321,10 @@ __global__ void fill_start_kernel(const GenArgs *inst, uint32_t y0, uint32_t id_
         p[x] = ones;
 }
 
-template <typename Id>
+template <typename Id, bool Slots>
 int launch_start_t(const StartArgs &b, uint32_t blocks, cudaStream_t s)
 {
-    auto kern = start_kernel<Id>;
+    auto kern = start_kernel<Id, Slots>;
     if (blocks == 0) {
         int dev = 0, sms = 0, per_sm = 0;
         cudaError_t e = cudaGetDevice(&dev);
@@ -338,10 +345,14 @@ int launch_start_t(const StartArgs &b, uint32_t blocks, cudaStream_t s)
 
 }  // namespace
 
-int launch_start(uint32_t id_bytes, const StartArgs &b, uint32_t blocks, cudaStream_t s)
+int launch_start(uint32_t id_bytes, const StartArgs &b, uint32_t blocks, cudaStream_t s,
+                 bool slots)
 {
-    return id_bytes == 8 ? launch_start_t<int64_t>(b, blocks, s)
-                         : launch_start_t<int32_t>(b, blocks, s);
+    if (slots)
+        return id_bytes == 8 ? launch_start_t<int64_t, true>(b, blocks, s)
+                             : launch_start_t<int32_t, true>(b, blocks, s);
+    return id_bytes == 8 ? launch_start_t<int64_t, false>(b, blocks, s)
+                         : launch_start_t<int32_t, false>(b, blocks, s);
 }
 
 int fill_start(uint32_t id_bytes, const GenArgs *d_inst, uint32_t count, uint64_t max_pairs,

@@ -39,12 +39,14 @@ PA_ERR_CAPACITY = 5
 PA_ERR_NOT_SUPPORTED = 6
 PA_ERR_BUSY = 7
 PA_ERR_NOT_FOUND = 8
+PA_ERR_IO = 9
 
 PA_SEED_STAR_REF = 0
 PA_SEED_CLIQUE = 1
 PA_MODEL_COPY = 0   # copy model (-A cuppa, -A scm)
 PA_MODEL_BA = 1     # repeated-nodes Barabasi-Albert (-A sba); STAR_REF seed only
 PA_LAYOUT_PAIRS = 0
+PA_LAYOUT_SLOTS = 1   # targets only: half the bytes; read out with write_edges / stream_edges
 PA_FORMAT_TEXT = 0
 PA_FORMAT_BINARY = 1
 
@@ -182,6 +184,11 @@ _SIGS = {
                                     ctypes.c_void_p]),
     "pa_write_edges": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_char_p,
                                       ctypes.c_int, ctypes.c_void_p]),
+    "pa_stream_edges": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_int,
+                                       ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p, _P(ctypes.c_uint64)]),
+    "pa_generate_to_file": (ctypes.c_int, [_P(PaParams), ctypes.c_char_p, ctypes.c_int,
+                                           _P(PaStats), _P(ctypes.c_uint64)]),
     "pa_write_degree_distribution": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p,
                                                     ctypes.c_char_p, ctypes.c_void_p]),
     "pa_batch_scratch_bytes": (ctypes.c_int, [_P(PaParams), ctypes.c_uint32,
@@ -249,14 +256,14 @@ def make_params(n: int, d: int, p: float, seed: int = 42, id_bits: int = 32,
                 seed_mode: int = PA_SEED_CLIQUE, blocks: int = 0, threads: int = 0,
                 tile_passes: int = 0, flags: int = 0, spin_limit_ns: int = 0,
                 start_nodes: int = 0, claim_tiles: int = 0,
-                model: int = 0) -> PaParams:
+                model: int = 0, layout: int = 0) -> PaParams:
     prm = PaParams()
     check(lib().pa_params_init(ctypes.byref(prm)), "pa_params_init")
     prm.n, prm.d, prm.p, prm.seed = n, d, float(p), seed
     prm.id_bits, prm.seed_mode = id_bits, seed_mode
     prm.blocks, prm.threads, prm.tile_passes = blocks, threads, tile_passes
     prm.flags, prm.spin_limit_ns, prm.start_nodes = flags, spin_limit_ns, start_nodes
-    prm.claim_tiles, prm.model = claim_tiles, model
+    prm.claim_tiles, prm.model, prm.layout = claim_tiles, model, layout
     return prm
 
 
@@ -286,10 +293,16 @@ def _stream_ptr(stream) -> int:
 
 
 def alloc_buffers(prm: PaParams, device=None):
-    """Device tensors for the edges (E x 2 ids) and the generation scratch."""
+    """Device tensors for the edges (E x 2 ids; SLOTS: (n-d-1) x d targets) and
+    the generation scratch."""
     torch = _torch()
     eb, sb = sizes(prm)
     dt = torch.int64 if prm.id_bits == 64 else torch.int32
+    if prm.layout == PA_LAYOUT_SLOTS:
+        rows = prm.n - prm.d - 1
+        edges = torch.empty((max(rows, 1), prm.d), dtype=dt, device=device or "cuda")
+        scratch = torch.empty(max(sb, 256), dtype=torch.uint8, device=device or "cuda")
+        return edges, scratch
     E = edge_count(prm)
     edges = torch.empty((max(E, 1), 2), dtype=dt, device=device or "cuda")
     scratch = torch.empty(max(sb, 256), dtype=torch.uint8, device=device or "cuda")
@@ -348,12 +361,15 @@ def trace(prm: PaParams, scratch, stream=None, max_samples: int = 2048):
 
 
 def generate(prm: PaParams, stream=None, raise_on_error: bool = True):
-    """Generate one graph; returns (edges tensor [E, 2] on the device, PaStats)."""
+    """Generate one graph; returns (edges tensor [E, 2] on the device, PaStats)
+    -- for PA_LAYOUT_SLOTS the targets [n-d-1, d] instead."""
     edges, scratch = alloc_buffers(prm)
     generate_into(prm, edges, scratch, stream)
     st = finish(scratch, stream)
     if raise_on_error:
         check(st.status, "pa_generate (device)")
+    if prm.layout == PA_LAYOUT_SLOTS:
+        return edges[: prm.n - prm.d - 1], st
     return edges[: edge_count(prm)], st
 
 
@@ -424,10 +440,44 @@ def build_csr(prm: PaParams, edges, stream=None):
 
 
 def write_edges(prm: PaParams, edges, path: str, binary: bool = False, stream=None) -> None:
-    """PAHelper::writeGraphToDisk's "u v" text (or raw pairs) from the device."""
+    """PAHelper::writeGraphToDisk's "u v" text (or raw pairs), formatted on the
+    device and streamed to the file (either layout)."""
     check(lib().pa_write_edges(ctypes.byref(prm), ctypes.c_void_p(edges.data_ptr()),
                                path.encode(), PA_FORMAT_BINARY if binary else PA_FORMAT_TEXT,
                                ctypes.c_void_p(_stream_ptr(stream))), "pa_write_edges")
+
+
+_SINK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64)
+
+
+def stream_edges(prm: PaParams, edges, sink, binary: bool = False, chunk_edges: int = 0,
+                 stream=None) -> int:
+    """pa_stream_edges: sink(bytes) receives the output in order (called from a
+    library thread); returns the byte count.  A sink that raises or returns a
+    true value stops the stream (PaError PA_ERR_IO)."""
+    def _cb(ctx, data, nbytes):
+        try:
+            return 1 if sink(ctypes.string_at(data, nbytes)) else 0
+        except Exception:
+            return 1
+    cb = _SINK(_cb)
+    total = ctypes.c_uint64()
+    check(lib().pa_stream_edges(ctypes.byref(prm), ctypes.c_void_p(edges.data_ptr()),
+                                PA_FORMAT_BINARY if binary else PA_FORMAT_TEXT, chunk_edges,
+                                ctypes.cast(cb, ctypes.c_void_p), None,
+                                ctypes.c_void_p(_stream_ptr(stream)), ctypes.byref(total)),
+          "pa_stream_edges")
+    return int(total.value)
+
+
+def generate_to_file(prm: PaParams, path: str, binary: bool = False):
+    """pa_generate_to_file: generate into library memory and write; returns
+    (PaStats, bytes written)."""
+    st, total = PaStats(), ctypes.c_uint64()
+    check(lib().pa_generate_to_file(ctypes.byref(prm), path.encode(),
+                                    PA_FORMAT_BINARY if binary else PA_FORMAT_TEXT,
+                                    ctypes.byref(st), ctypes.byref(total)), "pa_generate_to_file")
+    return st, int(total.value)
 
 
 def write_degree_distribution(prm: PaParams, edges, path: str, stream=None) -> None:

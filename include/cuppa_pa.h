@@ -37,7 +37,8 @@ typedef enum pa_status {
     PA_ERR_CAPACITY = 5,      /* a caller buffer is smaller than the call needs         */
     PA_ERR_NOT_SUPPORTED = 6, /* valid request this build does not handle               */
     PA_ERR_BUSY = 7,          /* server: admission refused for now (retry later)        */
-    PA_ERR_NOT_FOUND = 8      /* server: unknown or already released ticket             */
+    PA_ERR_NOT_FOUND = 8,     /* server: unknown or already released ticket             */
+    PA_ERR_IO = 9             /* a file could not be opened or written, or a sink failed */
 } pa_status;
 
 /* Seed graph on nodes 0..d.
@@ -53,7 +54,14 @@ enum { PA_SEED_STAR_REF = 0, PA_SEED_CLIQUE = 1 };
  *        d pairs at [S + (u-d-1)*d, S + (u-d)*d) in slot (generation) order.  Every
  *        pair is an edge with src > dst.  This is the reference's G[N][M] slot array
  *        (src/PA/cuPPA/cuPPA_1.cu:54) carried as an edge list. */
-enum { PA_LAYOUT_PAIRS = 0 };
+/* SLOTS: the targets alone -- node u = d+1..n-1 owns ids [(u-d-1)*d, (u-d)*d) in
+ *        slot order, the seed rows are implied by seed_mode and not stored.  Half
+ *        the bytes of PAIRS, so a graph twice as large stays resident; read it out
+ *        with pa_write_edges / pa_stream_edges, which emit the PAIRS order.  The
+ *        whole graph is generated by the start kernel, so n - d - 1 <= 2^31 and
+ *        start_nodes must be 0 (auto); other entry points that take an edge list
+ *        (CSR, canonicalize, batch, server) return PA_ERR_NOT_SUPPORTED. */
+enum { PA_LAYOUT_PAIRS = 0, PA_LAYOUT_SLOTS = 1 };
 
 /* pa_params.flags.  TEST_WITHHOLD_FIRST_TILE is for tests of the wait limit:
  * the generator never publishes its first tile, so every wait on that tile runs
@@ -324,12 +332,31 @@ uint64_t pa_sched_queued(const pa_sched *q);
 
 /* ---- files ------------------------------------------------------------------ */
 enum { PA_FORMAT_TEXT = 0, PA_FORMAT_BINARY = 1 };
-/* Write the device edge list to `path`: TEXT = one "u v" line per pair, the
- * format of PAHelper::writeGraphToDisk (src/PA/SPA/PAHelper.hpp:163-177; with
- * PA_SEED_STAR_REF also its row order); BINARY = raw little-endian id pairs.
- * Streams through pinned host buffers the call allocates and frees; waits. */
+/* Receives the output bytes in order; return 0 to go on, nonzero to stop (the
+ * call then returns PA_ERR_IO).  Called from a thread of the library, one call
+ * at a time; `data` is valid until the call returns. */
+typedef int (*pa_sink_fn)(void *ctx, const void *data, uint64_t bytes);
+
+/* Stream the graph in d_edges (either layout) to `sink`: TEXT = one "u v\n" line
+ * per edge, the format of PAHelper::writeGraphToDisk
+ * (src/PA/SPA/PAHelper.hpp:163-177; with PA_SEED_STAR_REF also its row order);
+ * BINARY = little-endian (src, dst) id pairs of id_bits each.  Order: the seed
+ * edges, then rows u = d+1..n-1 in slot order.  The text is formatted on the
+ * device; chunks of about chunk_edges edges (0 = 2^24) are copied to pinned host
+ * memory while the next chunk is formatted and the previous one is sunk.  Runs
+ * after the work already queued on `stream`; waits.  *bytes_out (optional) gets
+ * the byte count. */
+int pa_stream_edges(const pa_params *prm, const void *d_edges, int format, uint64_t chunk_edges,
+                    pa_sink_fn sink, void *ctx, void *stream, uint64_t *bytes_out);
+/* pa_stream_edges into the file `path` (created or truncated); waits. */
 int pa_write_edges(const pa_params *prm, const void *d_edges, const char *path, int format,
                    void *stream);
+/* Generate and write in one call (library-owned device memory, freed before
+ * return): with layout PA_LAYOUT_SLOTS the device holds only the targets, so
+ * graphs whose edge list is larger than the GPU's memory can be written.
+ * *stats (optional) as pa_generate_finish. */
+int pa_generate_to_file(const pa_params *prm, const char *path, int format, pa_stats *stats,
+                        uint64_t *bytes_out);
 /* Write the "Degree,Count" CSV of cuPPA::printDegreeDistribution
  * (src/PA/cuPPA/cuPPA.cu:103-165) for the graph in d_edges; degrees and their
  * histogram are computed on the device (temporaries allocated and freed with

@@ -38,8 +38,8 @@ def test_library_exports_every_declared_symbol(pa):
 
 def test_abi_version_and_strerror(pa):
     assert pa.lib().pa_abi_version() == 1
-    for s in range(0, 9):
-        assert pa.strerror(s)
+    for s in range(0, 10):
+        assert pa.strerror(s) != "unknown status"
     assert pa.strerror(0) == "ok"
 
 
@@ -121,3 +121,45 @@ def test_claim_tiles_and_model_checked(pa):
     assert pa.lib().pa_params_check(ctypes.byref(prm)) == pa.PA_ERR_INVALID
     prm = pa.make_params(1000, 4, 0.5, model=pa.PA_MODEL_BA, seed_mode=pa.PA_SEED_STAR_REF)
     assert pa.lib().pa_params_check(ctypes.byref(prm)) == pa.PA_OK
+
+
+@pytest.mark.parametrize("n,d,bits", [(100000, 4, 32), (10 ** 6, 32, 64), (6, 5, 32), (2 ** 31 + 5, 4, 64)])
+def test_slots_layout_sizes(pa, n, d, bits):
+    """SLOTS holds the targets alone: (n - d - 1) * d ids, half of PAIRS less the
+    seed rows; the edge count is the same graph's."""
+    prm = pa.make_params(n, d, 0.5, id_bits=bits, layout=pa.PA_LAYOUT_SLOTS)
+    eb, _ = pa.sizes(prm)
+    assert eb == (n - d - 1) * d * bits // 8
+    assert pa.edge_count(prm) == orc.edge_count(n, d, orc.SEED_CLIQUE)
+
+
+def test_slots_layout_limits(pa):
+    chk = pa.lib().pa_params_check
+    # the whole graph must fit the start kernel (n - d - 1 <= 2^31)
+    prm = pa.make_params(2 ** 31 + 6, 4, 0.5, id_bits=64, layout=pa.PA_LAYOUT_SLOTS)
+    assert chk(ctypes.byref(prm)) == pa.PA_ERR_NOT_SUPPORTED
+    prm = pa.make_params(10 ** 6, 4, 0.5, layout=pa.PA_LAYOUT_SLOTS, start_nodes=1000)
+    assert chk(ctypes.byref(prm)) == pa.PA_ERR_NOT_SUPPORTED
+    prm = pa.make_params(10 ** 6, 4, 0.5, layout=2)
+    assert chk(ctypes.byref(prm)) == pa.PA_ERR_NOT_SUPPORTED
+    # edge-list consumers refuse it without touching the device
+    prm = pa.make_params(10 ** 6, 4, 0.5, layout=pa.PA_LAYOUT_SLOTS)
+    rb, cb, sb = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+    assert pa.lib().pa_csr_bytes(ctypes.byref(prm), ctypes.byref(rb), ctypes.byref(cb),
+                                 ctypes.byref(sb)) == pa.PA_ERR_NOT_SUPPORTED
+    arr = (pa.PaParams * 1)(prm)
+    assert pa.lib().pa_batch_scratch_bytes(arr, 1, ctypes.byref(sb)) == pa.PA_ERR_NOT_SUPPORTED
+
+
+def test_stream_edges_rejects_bad_arguments(pa):
+    prm = pa.make_params(1000, 4, 0.5)
+    sink = pa._SINK(lambda ctx, data, n: 0)
+    total = ctypes.c_uint64()
+    L = pa.lib()
+    assert L.pa_stream_edges(ctypes.byref(prm), None, 0, 0, ctypes.cast(sink, ctypes.c_void_p),
+                             None, None, ctypes.byref(total)) == pa.PA_ERR_INVALID
+    assert L.pa_stream_edges(ctypes.byref(prm), ctypes.c_void_p(16), 7, 0,
+                             ctypes.cast(sink, ctypes.c_void_p), None, None,
+                             ctypes.byref(total)) == pa.PA_ERR_INVALID
+    assert L.pa_stream_edges(ctypes.byref(prm), ctypes.c_void_p(16), 0, 0, None, None, None,
+                             ctypes.byref(total)) == pa.PA_ERR_INVALID

@@ -403,6 +403,127 @@ def _edge_hash(torch, e):
     return int(((x * 0x9E3779B97F4A7C15 + idx * 0xC2B2AE3D27D4EB4F) ^ (x >> 7)).sum().item())
 
 
+STREAM_W = dict(n=2 ** 30, d=4, p=0.5, seed=1234, id_bits=64, seed_mode=CLIQUE,
+                name="copy-model PA, n=2^30, d=4, p=0.5, int64 ids, clique seed, Philox seed "
+                     "1234, SLOTS layout, written as 'u v' text")
+STREAM_REF_NODES = 2 ** 22      # reference sample per step: scm generation + its writer
+
+
+def d2h_link_gbs(torch, nbytes=1 << 30, reps=5) -> float:
+    """Plain pinned device->host copy bandwidth (the host link's roofline)."""
+    src = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    dst = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    s = torch.cuda.Stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(s):
+        dst.copy_(src, non_blocking=True)
+        a.record(s)
+        for _ in range(reps):
+            dst.copy_(src, non_blocking=True)
+        b.record(s)
+    s.synchronize()
+    return nbytes * reps / (a.elapsed_time(b) / 1e3) / 1e9
+
+
+def stream_chunks(n, d, chunk_edges=1 << 24) -> int:
+    """Chunks pa_stream_edges cuts rows d+1..n-1 into (whole tiles of 2048 // d rows)."""
+    rows, tile_rows = n - d - 1, 2048 // d
+    chunk_rows = -(-max(1, chunk_edges // d) // tile_rows) * tile_rows
+    return -(-rows // min(chunk_rows, rows))
+
+
+def run_stream(args):
+    """Generation into the targets-only layout, then the edge list as text,
+    formatted on the device and copied out in chunks to a discarding sink."""
+    import ctypes
+    import torch
+    import cuppa_b200 as pa
+
+    torch.cuda.set_device(0)
+    w = STREAM_W
+    prm = pa.make_params(w["n"], w["d"], w["p"], seed=w["seed"], id_bits=w["id_bits"],
+                         seed_mode=w["seed_mode"], layout=pa.PA_LAYOUT_SLOTS)
+    E = pa.edge_count(prm)
+    slots, scratch = pa.alloc_buffers(prm)
+    stream = torch.cuda.Stream()
+    discard = pa._SINK(lambda ctx, data, nbytes: 0)
+    total = ctypes.c_uint64()
+
+    def step():
+        pa.generate_into(prm, slots, scratch, stream)
+        pa.check(pa.finish(scratch, stream).status, "generation")
+        t0 = time.perf_counter()
+        pa.check(pa.lib().pa_stream_edges(ctypes.byref(prm), ctypes.c_void_p(slots.data_ptr()),
+                                          pa.PA_FORMAT_TEXT, 0,
+                                          ctypes.cast(discard, ctypes.c_void_p), None,
+                                          ctypes.c_void_p(stream.cuda_stream),
+                                          ctypes.byref(total)), "pa_stream_edges")
+        return time.perf_counter() - t0
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clk:
+        t0 = time.perf_counter()
+        stream_s = [step() for _ in range(args.steps)]
+        t_all = time.perf_counter() - t0
+    text_bytes = int(total.value)
+    del slots, scratch
+    torch.cuda.empty_cache()
+    link = d2h_link_gbs(torch)
+    # end to end: the one call a user makes (library memory, generate, write the file)
+    t0 = time.perf_counter()
+    st, nbytes = pa.generate_to_file(prm, "/dev/null")
+    e2e_s = time.perf_counter() - t0
+    pa.check(st.status, "pa_generate_to_file")
+    achieved = text_bytes / statistics.mean(stream_s) / 1e9
+    line = {
+        "metric": "edges/s generated and written as text (copy-model PA)",
+        "value": E * args.steps / t_all, "unit": "edges/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_all / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (generator parameters only; output is the graph's text)",
+        "config": {"workload": w["name"], "edges": E, "text_bytes": text_bytes,
+                   "sink": "discard (host memory, native callback)",
+                   "timing": "host clock around generate + finish + pa_stream_edges"},
+        "roofline": {"bound": "host link (D2H)", "achieved": achieved, "peak": link,
+                     "unit": "GB/s", "frac": achieved / link, "peak_source": "measured in run",
+                     "traffic": None, "kernel": "pa_stream_edges pipeline",
+                     "stream_ms_mean": 1e3 * statistics.mean(stream_s)},
+        "e2e": {"value": E / e2e_s, "unit": "edges/s", "h2d_bytes_per_step": 80,
+                "d2h_bytes_per_step": nbytes,
+                "call": "pa_generate_to_file(prm, '/dev/null', TEXT): alloc, generate, write, free"},
+        # per step: the start kernel, then 3 formatting kernels per chunk
+        "gpu_launches": (1 + 3 * stream_chunks(w["n"], w["d"])) * args.steps,
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = reference_writer_sample(STREAM_REF_NODES, w["d"], w["p"])
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def reference_writer_sample(n, d, p):
+    """The reference's sequential path for the same job on one core: -A scm
+    generation (scm_ref) plus PAHelper::writeGraphToDisk (write_ref), n nodes."""
+    scm = os.path.join(ROOT, "oracle", "_ref", "scm_ref")
+    wr = os.path.join(ROOT, "oracle", "_ref", "write_ref")
+    if not (os.path.exists(scm) and os.path.exists(wr)):
+        return None
+    with tempfile.TemporaryDirectory() as td:
+        out = subprocess.run([scm, str(n), str(d), str(p), td, "-"], cwd=td,
+                             capture_output=True, text=True, check=True).stdout
+        t_gen = [float(x.split(":")[1]) for x in out.splitlines()
+                 if x.startswith("Computation Time")][0]
+        out = subprocess.run([wr, str(n), str(d), str(p), "/dev/null"], capture_output=True,
+                             text=True, check=True).stdout
+        t_wr = [float(x.split(":")[1]) for x in out.splitlines() if x.startswith("Write Time")][0]
+    edges = (n - d) * d
+    return {"value": edges / (t_gen + t_wr), "unit": "edges/s", "cores": 1, "kind": "reference",
+            "sample": f"reference -A scm generation ({t_gen:.2f} s) + PAHelper::writeGraphToDisk "
+                      f"to /dev/null ({t_wr:.2f} s), n={n}, d={d}, p={p}, int32, one thread"}
+
+
 def run_batched(args):
     """4,096 mixed instances: one persistent launch per wave vs one launch per
     graph, identical outputs checked by digest; graphs/s of both."""
@@ -579,7 +700,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched", "served"],
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched", "served", "stream"],
                     default="c3")
     ap.add_argument("--tile-passes", type=int, default=0)
     ap.add_argument("--blocks", type=int, default=0)
@@ -598,6 +719,30 @@ def main():
         return run_batched(args)
     if args.workload == "served":
         return run_served(args)
+    if args.workload == "stream":
+        if args.impl == "reference":
+            world, rank, _ = dist_setup()
+            if rank != 0:
+                return 0
+            samples = [reference_writer_sample(STREAM_REF_NODES, STREAM_W["d"], STREAM_W["p"])
+                       for _ in range(args.warmup + args.steps)][args.warmup:]
+            if samples[0] is None:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "oracle/_ref/scm_ref or write_ref not built"}))
+                return 0
+            v = statistics.mean(x["value"] for x in samples)
+            print(json.dumps({"impl": "reference", "metric": "edges/s generated and written as "
+                              "text (copy-model PA)", "value": v, "unit": "edges/s",
+                              "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                              "dtype": "int32", "data": "synthetic",
+                              "config": {"workload": STREAM_W["name"],
+                                         "sample_nodes": STREAM_REF_NODES},
+                              "cpu_baseline": samples[-1],
+                              "e2e": {"value": v, "unit": "edges/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}), flush=True)
+            return 0
+        return run_stream(args)
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
         return run_reference(args, w)

@@ -14,6 +14,9 @@ Two kinds of fixture:
    oracle/_ref/sba_ref is the reference's repeated-nodes BA (-A sba,
    src/PA/SPA/SerialBA.cpp, same seed 5489); its "Degree,Count" CSVs
    (src/PA/SPA/PAHelper.hpp:69-147) pin the oracle's BA model in MT_REF mode.
+   oracle/_ref/write_ref runs the reference's edge-list writer
+   (PAHelper::writeGraphToDisk, src/PA/SPA/PAHelper.hpp:163-177) on the
+   oracle's MT_REF star-seed graph; its file pins the text format and row order.
 2. Oracle digests.  FNV-1a 64 of the oracle's Philox-mode edge lists (slot
    order and canonical, int64 little-endian) for a fixed list of shapes, plus one
    tiny full edge list.  They pin the oracle itself across edits.
@@ -122,6 +125,18 @@ def ba_digest_fixtures():
                    "cases": cases}, f, indent=1)
 
 
+WRITE_RUN = (2000, 3, 0.5)
+
+
+def write_fixture():
+    ref = os.path.join(orc.ORACLE_DIR, "_ref", "write_ref")
+    if not os.path.exists(ref):
+        raise SystemExit(f"{ref} missing: run `make -C oracle ref` first")
+    n, m, p = WRITE_RUN
+    out = os.path.join(HERE, f"ref_write_n{n}_m{m}_p{p}.txt")
+    subprocess.run([ref, str(n), str(m), str(p), out], check=True, stdout=subprocess.DEVNULL)
+
+
 def digest_fixtures():
     cases = []
     for n, d, p, seed, mode in DIGEST_CASES:
@@ -148,6 +163,7 @@ def digest_fixtures():
 if __name__ == "__main__":
     scm_fixtures()
     sba_fixtures()
+    write_fixture()
     digest_fixtures()
     ba_digest_fixtures()
     print("fixtures written to", HERE)

@@ -316,3 +316,14 @@ def test_ba_rejects_bad_shapes():
         orc.generate_ba(4, 4, 1)
     with pytest.raises(ValueError):
         orc.generate_ba(10, 0, 1)
+
+
+def test_text_format_is_the_reference_writers():
+    """The reference's PAHelper::writeGraphToDisk, run on the oracle's MT_REF
+    graph (tests/golden/ref_write_*.txt), writes exactly the "u v" lines of the
+    PAIRS order with the reference seed: node M's star row, then rows M+1..N-1."""
+    n, m, p = 2000, 3, 0.5
+    G = orc.generate(n, m, p, 5489, orc.SEED_STAR_REF, orc.RNG_MT_REF)
+    text = "".join(f"{u} {v}\n" for u, v in orc.pairs_slot_order(G, orc.SEED_STAR_REF).tolist())
+    with open(os.path.join(GOLD, f"ref_write_n{n}_m{m}_p{p}.txt")) as f:
+        assert text == f.read()

@@ -318,6 +318,101 @@ struct Writer {
     }
 };
 
+// Staging memory kept between calls.  Pinning a few hundred MB of host memory
+// and freeing it again (which waits for the device) cost ~0.3 s per call, a
+// sixth of a 2^30-node text write; the buffers grow to the largest request and
+// stay until pa_stream_trim.  One call at a time uses the cached set; a
+// concurrent call allocates its own.
+struct Staging {
+    int device = -1;
+    void *host[2] = {nullptr, nullptr};
+    uint64_t host_bytes = 0;
+    void *dev[2] = {nullptr, nullptr};
+    uint64_t dev_bytes = 0;
+    void *meta = nullptr;
+    uint64_t meta_bytes = 0;
+    unsigned long long *h_total = nullptr;
+
+    void free_all()
+    {
+        for (int i = 0; i < 2; ++i) {
+            if (host[i]) cudaFreeHost(host[i]);
+            if (dev[i]) cudaFree(dev[i]);
+            host[i] = dev[i] = nullptr;
+        }
+        if (meta) cudaFree(meta);
+        if (h_total) cudaFreeHost(h_total);
+        meta = nullptr;
+        h_total = nullptr;
+        host_bytes = dev_bytes = meta_bytes = 0;
+    }
+};
+
+std::mutex g_stage_mu;
+Staging g_stage;
+bool g_stage_busy = false;
+
+// Take the cached set (or an empty one) and grow it to the sizes asked.
+cudaError_t stage_acquire(Staging &S, bool &cached, uint64_t host_bytes, uint64_t dev_bytes,
+                          uint64_t meta_bytes)
+{
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    {
+        std::lock_guard<std::mutex> lk(g_stage_mu);
+        cached = !g_stage_busy;
+        if (cached) {
+            g_stage_busy = true;
+            if (g_stage.device == device) S = g_stage;
+            else g_stage.free_all();   // cached for another device: let it go
+            g_stage = Staging();
+        }
+    }
+    if (S.device != device) S = Staging();   // nothing cached for this device
+    S.device = device;
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+        if (S.host_bytes < host_bytes) {
+            if (S.host[i]) cudaFreeHost(S.host[i]);
+            S.host[i] = nullptr;
+            e = cudaMallocHost(&S.host[i], host_bytes);
+        }
+        if (e == cudaSuccess && S.dev_bytes < dev_bytes) {
+            if (S.dev[i]) cudaFree(S.dev[i]);
+            S.dev[i] = nullptr;
+            e = cudaMalloc(&S.dev[i], dev_bytes);
+        }
+    }
+    if (e == cudaSuccess) {
+        S.host_bytes = std::max(S.host_bytes, host_bytes);
+        S.dev_bytes = std::max(S.dev_bytes, dev_bytes);
+    }
+    if (e == cudaSuccess && S.meta_bytes < meta_bytes) {
+        if (S.meta) cudaFree(S.meta);
+        S.meta = nullptr;
+        e = cudaMalloc(&S.meta, meta_bytes);
+        if (e == cudaSuccess) S.meta_bytes = meta_bytes;
+    }
+    if (e == cudaSuccess && !S.h_total)
+        e = cudaMallocHost(reinterpret_cast<void **>(&S.h_total), 2 * sizeof(unsigned long long));
+    return e;
+}
+
+void stage_release(Staging &S, bool cached, bool keep)
+{
+    if (cached && keep) {
+        std::lock_guard<std::mutex> lk(g_stage_mu);
+        g_stage = S;
+        g_stage_busy = false;
+        return;
+    }
+    S.free_all();
+    if (cached) {
+        std::lock_guard<std::mutex> lk(g_stage_mu);
+        g_stage_busy = false;
+    }
+}
+
 }  // namespace
 
 int stream_edges(const pa_params *prm, const GenPlan &p, const void *d_edges, int format,
@@ -376,20 +471,22 @@ int stream_edges(const pa_params *prm, const GenPlan &p, const void *d_edges, in
     Writer W;
     W.sink = sink;
     W.ctx = ctx;
-    unsigned char *stage[2] = {nullptr, nullptr};
-    unsigned long long *meta = nullptr;   // 2 x (tiles_cap tile counts + 1 total)
-    unsigned long long *h_total = nullptr;
+    Staging St;
+    bool cached = false;
+    cudaError_t e = stage_acquire(St, cached, chunk_cap, direct ? 0 : chunk_cap,
+                                  text ? 2 * (tiles_cap + 1) * sizeof(unsigned long long) : 0);
+    unsigned char *stage[2] = {(unsigned char *)St.dev[0], (unsigned char *)St.dev[1]};
+    unsigned long long *meta = (unsigned long long *)St.meta;   // 2 x (tile counts + 1 total)
+    unsigned long long *h_total = St.h_total;
+    W.buf[0] = St.host[0];
+    W.buf[1] = St.host[1];
     cudaEvent_t formatted[2] = {nullptr, nullptr};
     cudaStream_t cs = nullptr;
-    cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
     for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
-        e = cudaMallocHost(&W.buf[i], chunk_cap);
-        if (e == cudaSuccess && !direct) e = cudaMalloc(&stage[i], chunk_cap);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&W.copied[i], cudaEventDisableTiming);
+        e = cudaEventCreateWithFlags(&W.copied[i], cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&formatted[i], cudaEventDisableTiming);
     }
-    if (e == cudaSuccess && text) e = cudaMalloc(&meta, 2 * (tiles_cap + 1) * sizeof(unsigned long long));
-    if (e == cudaSuccess && text) e = cudaMallocHost(&h_total, 2 * sizeof(unsigned long long));
 
     std::thread writer;
     int rc = PA_OK;
@@ -476,13 +573,10 @@ int stream_edges(const pa_params *prm, const GenPlan &p, const void *d_edges, in
     if (e == cudaSuccess) e = e3;
     if (e == cudaSuccess) e = W.cuda;
     for (int i = 0; i < 2; ++i) {
-        if (W.buf[i]) cudaFreeHost(W.buf[i]);
-        if (stage[i]) cudaFree(stage[i]);
         if (W.copied[i]) cudaEventDestroy(W.copied[i]);
         if (formatted[i]) cudaEventDestroy(formatted[i]);
     }
-    if (meta) cudaFree(meta);
-    if (h_total) cudaFreeHost(h_total);
+    stage_release(St, cached, e == cudaSuccess);
     if (e != cudaSuccess) return set_cuda_error(e);
     if (rc == PA_OK) rc = W.status;
     if (rc == PA_OK && bytes_out) *bytes_out = written;
@@ -513,6 +607,15 @@ int pa_stream_edges(const pa_params *prm, const void *d_edges, int format, uint6
     if (!d_edges && prm->n > p.u_first) return PA_ERR_INVALID;
     return stream_edges(prm, p, d_edges, format, chunk_edges, sink, ctx, (cudaStream_t)stream,
                         bytes_out);
+}
+
+int pa_stream_trim(void)
+{
+    std::lock_guard<std::mutex> lk(g_stage_mu);
+    if (g_stage_busy) return PA_ERR_BUSY;
+    g_stage.free_all();
+    g_stage = Staging();
+    return PA_OK;
 }
 
 int pa_write_edges(const pa_params *prm, const void *d_edges, const char *path, int format,

@@ -187,6 +187,7 @@ _SIGS = {
     "pa_stream_edges": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_int,
                                        ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p,
                                        ctypes.c_void_p, _P(ctypes.c_uint64)]),
+    "pa_stream_trim": (ctypes.c_int, []),
     "pa_generate_to_file": (ctypes.c_int, [_P(PaParams), ctypes.c_char_p, ctypes.c_int,
                                            _P(PaStats), _P(ctypes.c_uint64)]),
     "pa_write_degree_distribution": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p,
@@ -468,6 +469,11 @@ def stream_edges(prm: PaParams, edges, sink, binary: bool = False, chunk_edges: 
                                 ctypes.c_void_p(_stream_ptr(stream)), ctypes.byref(total)),
           "pa_stream_edges")
     return int(total.value)
+
+
+def stream_trim() -> None:
+    """Free the staging memory pa_stream_edges keeps between calls."""
+    check(lib().pa_stream_trim(), "pa_stream_trim")
 
 
 def generate_to_file(prm: PaParams, path: str, binary: bool = False):

@@ -348,6 +348,10 @@ typedef int (*pa_sink_fn)(void *ctx, const void *data, uint64_t bytes);
  * the byte count. */
 int pa_stream_edges(const pa_params *prm, const void *d_edges, int format, uint64_t chunk_edges,
                     pa_sink_fn sink, void *ctx, void *stream, uint64_t *bytes_out);
+/* pa_stream_edges keeps its staging memory (two pinned host buffers and two
+ * device buffers of one chunk each) for the next call on the same device;
+ * pa_stream_trim frees it (PA_ERR_BUSY while a stream is running). */
+int pa_stream_trim(void);
 /* pa_stream_edges into the file `path` (created or truncated); waits. */
 int pa_write_edges(const pa_params *prm, const void *d_edges, const char *path, int format,
                    void *stream);

@@ -147,3 +147,20 @@ def test_slots_degrees_and_dd(pa, cuda_ok, tmp_path):
     pa.write_degree_distribution(prm, S, path)
     with open(path) as f:
         assert f.read() == orc.dd_csv_from_degrees(orc.degrees(G, mode))
+
+
+def test_staging_cache_grows_and_trims(pa, cuda_ok):
+    """A small stream, a larger one (the cached buffers grow), then trim; the
+    outputs are unaffected by what the cache held before."""
+    small = pa.make_params(3000, 4, 0.5, seed=1, layout=pa.PA_LAYOUT_SLOTS)
+    big = pa.make_params(300000, 8, 0.5, seed=2, layout=pa.PA_LAYOUT_SLOTS)
+    Es, _ = pa.generate(small)
+    Eb, _ = pa.generate(big)
+    want_s = text_of(oracle_pairs(3000, 4, 0.5, 1, 1)[1])
+    assert collect(pa, small, Es) == want_s
+    out_b = collect(pa, big, Eb, chunk_edges=1 << 18)
+    assert out_b == text_of(oracle_pairs(300000, 8, 0.5, 2, 1)[1])
+    assert collect(pa, small, Es) == want_s
+    pa.stream_trim()
+    assert collect(pa, small, Es, binary=True) == collect(pa, small, Es, binary=True)
+    pa.stream_trim()

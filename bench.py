@@ -524,16 +524,39 @@ def reference_writer_sample(n, d, p):
                       f"to /dev/null ({t_wr:.2f} s), n={n}, d={d}, p={p}, int32, one thread"}
 
 
+def rank_share(pa, prms, world: int, rank: int) -> list:
+    """Instances this rank generates: its part of pa_batch_partition (largest
+    first, each to the lightest part), the same split on every rank."""
+    if world == 1:
+        return list(range(len(prms)))
+    part = pa.batch_partition(prms, world)
+    return [i for i, p in enumerate(part) if p == rank]
+
+
 def run_batched(args):
     """4,096 mixed instances: one persistent launch per wave vs one launch per
-    graph, identical outputs checked by digest; graphs/s of both."""
+    graph, identical outputs checked by digest; graphs/s of both.  With N ranks
+    the instances are split by pa_batch_partition and each rank runs its part
+    (the total is fixed: strong scaling; no collective beyond the timing)."""
     import torch
+    import torch.distributed as dist
     import cuppa_b200 as pa
     from cuppa_b200.workloads import batched_instances, edges_of
 
-    torch.cuda.set_device(0)
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
     inst = batched_instances(args.instances)
-    order = sorted(range(len(inst)), key=lambda i: -edges_of(inst[i]["n"], inst[i]["d"]))
+
+    def prm(i):
+        x = inst[i]
+        return pa.make_params(x["n"], x["d"], x["p"], seed=x["seed"], id_bits=32,
+                              seed_mode=pa.PA_SEED_CLIQUE)
+
+    mine = rank_share(pa, [prm(i) for i in range(len(inst))], world, rank)
+    order = sorted(mine, key=lambda i: -edges_of(inst[i]["n"], inst[i]["d"]))
     budget = int(args.budget_gb * 1e9)
     waves, cur, used = [], [], 0
     for i in order:
@@ -545,11 +568,6 @@ def run_batched(args):
         used += b
     if cur:
         waves.append(cur)
-
-    def prm(i):
-        x = inst[i]
-        return pa.make_params(x["n"], x["d"], x["p"], seed=x["seed"], id_bits=32,
-                              seed_mode=pa.PA_SEED_CLIQUE)
 
     stream = torch.cuda.Stream()
     t_batch = t_plain = 0.0
@@ -588,15 +606,28 @@ def run_batched(args):
             torch.cuda.empty_cache()
     same = all(digests_b[i] == digests_p[i] for i in digests_b)
     n_graphs = len(inst)
+    t_batch = max_over_ranks(t_batch, world, "cuda")
+    t_plain = max_over_ranks(t_plain, world, "cuda")
+    if world > 1:
+        flags = torch.tensor([0.0 if same else 1.0, float(total_edges)], device="cuda")
+        dist.all_reduce(flags)
+        same, total_edges = flags[0].item() == 0.0, int(flags[1].item())
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0 if same else 1
     line = {
         "metric": "graphs/s, batched mixed instances (one persistent launch per wave)",
-        "value": n_graphs / t_batch, "unit": "graphs/s", "n_gpus": 1, "steps": 1,
+        "value": n_graphs / t_batch, "unit": "graphs/s", "n_gpus": world, "steps": 1,
         "warmup": args.warmup, "ms_per_step": t_batch * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "scaling": "strong", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (generator parameters only)",
         "config": {"workload": f"{n_graphs} instances: n=round(10^U(3,7)), d=U{{1..32}}, "
                                "p=U(0.1,0.9), seed=1000+i, int32, clique seed",
-                   "edges": total_edges, "waves": len(waves), "wave_budget_gb": args.budget_gb},
+                   "edges": total_edges, "waves_rank0": len(waves),
+                   "wave_budget_gb": args.budget_gb,
+                   "parallelism": f"instances split over {world} ranks (pa_batch_partition)"
+                   if world > 1 else "single"},
         "plain_graphs_per_s": n_graphs / t_plain, "plain_ms": t_plain * 1e3,
         "speedup_vs_plain": t_plain / t_batch, "identical_outputs": same,
         "edges_per_s_batched": total_edges / t_batch,

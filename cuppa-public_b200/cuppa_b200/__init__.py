@@ -213,6 +213,21 @@ _SIGS = {
                                       ctypes.c_void_p, ctypes.c_uint64, _P(ctypes.c_void_p)]),
     "pa_plan_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "pa_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "pa_router_create": (ctypes.c_int, [_P(PaServerConfig), _P(ctypes.c_int32), ctypes.c_uint32,
+                                        _P(ctypes.c_void_p)]),
+    "pa_router_submit": (ctypes.c_int, [ctypes.c_void_p, _P(PaParams), _P(ctypes.c_uint64)]),
+    "pa_router_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _P(PaResult)]),
+    "pa_router_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                      _P(PaResult)]),
+    "pa_router_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    "pa_router_device_of": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _P(ctypes.c_int32)]),
+    "pa_router_stats_get": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, _P(PaServerStats)]),
+    "pa_router_size": (ctypes.c_uint32, [ctypes.c_void_p]),
+    "pa_router_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "pa_route_pick": (ctypes.c_uint32, [_P(ctypes.c_uint64), _P(ctypes.c_uint64), ctypes.c_uint32,
+                                        ctypes.c_uint64]),
+    "pa_batch_partition": (ctypes.c_int, [_P(PaParams), ctypes.c_uint32, ctypes.c_uint32,
+                                          _P(ctypes.c_uint32)]),
     "pa_sched_create": (ctypes.c_void_p, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32]),
     "pa_sched_destroy": (None, [ctypes.c_void_p]),
     "pa_sched_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
@@ -747,3 +762,86 @@ class Server:
                               device="cuda")
         return rp, col
 
+
+
+# ---------------------------------------------------------------------------
+# Several GPUs: request router and batch partition
+# ---------------------------------------------------------------------------
+def route_pick(load_bytes, budget_bytes, request_bytes: int) -> int:
+    """pa_route_pick: the server index a request of request_bytes goes to."""
+    n = len(load_bytes)
+    lo = (ctypes.c_uint64 * n)(*load_bytes)
+    bu = (ctypes.c_uint64 * n)(*budget_bytes)
+    return int(lib().pa_route_pick(lo, bu, n, request_bytes))
+
+
+def batch_partition(prms, k: int) -> list:
+    """pa_batch_partition: part index (0..k-1) of every instance, LPT by edge bytes."""
+    arr = (PaParams * len(prms))(*prms)
+    out = (ctypes.c_uint32 * max(len(prms), 1))()
+    check(lib().pa_batch_partition(arr, len(prms), k, out), "pa_batch_partition")
+    return list(out)[: len(prms)]
+
+
+class Router:
+    """One request server per device behind one ticket space (pa_router_*)."""
+
+    def __init__(self, devices, budget_bytes: int = 0, max_batch: int = 0,
+                 max_inflight: int = 0, max_queue: int = 0, ttl_ns: int = 0,
+                 aging_ns: int = 0, outputs: int = 0):
+        cfg = PaServerConfig()
+        check(lib().pa_server_config_init(ctypes.byref(cfg)), "pa_server_config_init")
+        cfg.budget_bytes, cfg.max_batch, cfg.max_inflight = budget_bytes, max_batch, max_inflight
+        cfg.max_queue, cfg.ttl_ns, cfg.aging_ns, cfg.outputs = max_queue, ttl_ns, aging_ns, outputs
+        devs = (ctypes.c_int32 * len(devices))(*devices)
+        h = ctypes.c_void_p()
+        check(lib().pa_router_create(ctypes.byref(cfg), devs, len(devices), ctypes.byref(h)),
+              "pa_router_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pa_router_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __len__(self):
+        return int(lib().pa_router_size(self._h))
+
+    def submit(self, prm: PaParams) -> int:
+        t = ctypes.c_uint64()
+        check(lib().pa_router_submit(self._h, ctypes.byref(prm), ctypes.byref(t)),
+              "pa_router_submit")
+        return int(t.value)
+
+    def poll(self, ticket: int):
+        r = PaResult()
+        return lib().pa_router_poll(self._h, ticket, ctypes.byref(r)), r
+
+    def wait(self, ticket: int, timeout_ns: int = 0):
+        r = PaResult()
+        return lib().pa_router_wait(self._h, ticket, timeout_ns, ctypes.byref(r)), r
+
+    def release(self, ticket: int) -> int:
+        return lib().pa_router_release(self._h, ticket)
+
+    def device_of(self, ticket: int) -> int:
+        d = ctypes.c_int32()
+        check(lib().pa_router_device_of(self._h, ticket, ctypes.byref(d)), "pa_router_device_of")
+        return int(d.value)
+
+    def server_of(self, ticket: int) -> int:
+        return ticket & 0xFF
+
+    def stats(self, index=None) -> PaServerStats:
+        st = PaServerStats()
+        i = len(self) if index is None else index
+        check(lib().pa_router_stats_get(self._h, i, ctypes.byref(st)), "pa_router_stats_get")
+        return st

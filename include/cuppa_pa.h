@@ -330,6 +330,37 @@ int pa_sched_release(pa_sched *q, uint64_t ticket, uint64_t bytes);
 uint64_t pa_sched_in_use(const pa_sched *q);
 uint64_t pa_sched_queued(const pa_sched *q);
 
+/* ---- several GPUs: router and batch partition ------------------------------- */
+/* One graph never spans GPUs (any copy read may land on any earlier node), so
+ * more GPUs serve more graphs.  A router owns one request server per device
+ * (cfg copied, cfg.device replaced) and places each request on the server whose
+ * routed, unreleased bytes (edge list, plus CSR arrays with PA_OUT_CSR) would be
+ * the smallest fraction of its budget (pa_route_pick).  Its tickets name the
+ * server; poll / wait / release behave as pa_server_*.  No data moves between
+ * GPUs.  At most 255 devices; a device may be listed more than once. */
+typedef struct pa_router pa_router;
+int pa_router_create(const pa_server_config *cfg, const int32_t *devices, uint32_t n_devices,
+                     pa_router **out);
+int pa_router_submit(pa_router *r, const pa_params *prm, uint64_t *ticket);
+int pa_router_poll(pa_router *r, uint64_t ticket, pa_result *out);
+int pa_router_wait(pa_router *r, uint64_t ticket, uint64_t timeout_ns, pa_result *out);
+int pa_router_release(pa_router *r, uint64_t ticket);
+/* The CUDA device whose memory holds the ticket's result. */
+int pa_router_device_of(pa_router *r, uint64_t ticket, int32_t *device);
+/* Statistics of server `index` (0..size-1), or summed over all with index == size. */
+int pa_router_stats_get(pa_router *r, uint32_t index, pa_server_stats *out);
+uint32_t pa_router_size(const pa_router *r);
+int pa_router_destroy(pa_router *r);
+/* The placement rule alone (host arithmetic): the index i minimising
+ * (load_bytes[i] + request_bytes) / budget_bytes[i], exactly; ties go to the
+ * lowest index. */
+uint32_t pa_route_pick(const uint64_t *load_bytes, const uint64_t *budget_bytes, uint32_t n,
+                       uint64_t request_bytes);
+/* Split a batch over k parts (one per GPU / process): instances largest first
+ * (edge bytes), each to the part with the fewest bytes so far, ties to the lowest
+ * part; part_of[i] in [0, k).  Deterministic: every process gets the same split. */
+int pa_batch_partition(const pa_params *prms, uint32_t count, uint32_t k, uint32_t *part_of);
+
 /* ---- files ------------------------------------------------------------------ */
 enum { PA_FORMAT_TEXT = 0, PA_FORMAT_BINARY = 1 };
 /* Receives the output bytes in order; return 0 to go on, nonzero to stop (the

@@ -4,14 +4,17 @@
 //   cuppa_runner -A cuppa -n 100000 -x 4 -a 0.5 [--seed 42] [--id-bits 32]
 //                [--seed-mode clique|star] [-b blocks] [-t threads] [-s stages]
 //                [--show-dd 1 --dd-filename dd.csv] [-o outdir]
-//                [--out edges.txt --format text|binary] [--csr]
+//                [--out edges.txt --format text|binary] [--csr] [--layout pairs|slots]
 //
 // -A cuppa and -A cuppa-adaptive both run the copy model (-s is accepted and
 // ignored: there are no stages); -A scm is the same model with the reference's
 // star seed (src/PA/SPA/SerialCopyModel3.cpp); -A sba is the repeated-nodes
-// Barabasi-Albert model (src/PA/SPA/SerialBA.cpp), star seed, -a ignored.  Prints "Computation Time: <s>"
-// like the reference (src/PA/cuPPA/cuPPA_1.cu:511) plus the device counters.
-// Errors are reported with their pa_strerror text and exit status 1.
+// Barabasi-Albert model (src/PA/SPA/SerialBA.cpp), star seed, -a ignored.
+// Prints "Computation Time: <s>" like the reference (src/PA/cuPPA/cuPPA_1.cu:511)
+// plus the device counters.
+// --layout slots keeps only the targets on the device (half the bytes; --out and
+// --show-dd work on it, --csr does not).  Errors are reported with their
+// pa_strerror text and exit status 1.
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -30,7 +33,7 @@ void usage()
                  "usage: cuppa_runner -A cuppa|cuppa-adaptive|scm|sba -n N -x M -a P [--seed S]\n"
                  "       [--id-bits 32|64] [--seed-mode clique|star] [-b B] [-t T] [-s S]\n"
                  "       [--show-dd 0|1] [--dd-filename F] [-o DIR] [--out FILE]\n"
-                 "       [--format text|binary] [--csr]\n");
+                 "       [--format text|binary] [--csr] [--layout pairs|slots]\n");
 }
 
 int fail(const char *what, int rc)
@@ -76,6 +79,7 @@ int main(int argc, char **argv)
         else if (a == "--out") out = val();
         else if (a == "--format") format = val();
         else if (a == "--csr") csr = true;
+        else if (a == "--layout") prm.layout = std::string(val()) == "slots" ? PA_LAYOUT_SLOTS : PA_LAYOUT_PAIRS;
         else if (a == "-h" || a == "--help") { usage(); return 0; }
         else { usage(); return 2; }
     }

@@ -164,3 +164,17 @@ def test_staging_cache_grows_and_trims(pa, cuda_ok):
     pa.stream_trim()
     assert collect(pa, small, Es, binary=True) == collect(pa, small, Es, binary=True)
     pa.stream_trim()
+
+
+def test_runner_writes_slots_graph(cuda_ok, tmp_path):
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    runner = os.path.join(root, "cuppa-public_b200", "bin", "cuppa_runner")
+    out = str(tmp_path / "g.txt")
+    r = subprocess.run([runner, "-A", "scm", "-n", "30000", "-x", "4", "-a", "0.5", "--seed", "5",
+                        "--layout", "slots", "--out", out], capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 0, r.stderr
+    G = orc.generate(30000, 4, 0.5, 5, orc.SEED_STAR_REF)
+    with open(out, "rb") as f:
+        assert f.read() == text_of(orc.pairs_slot_order(G, orc.SEED_STAR_REF))

@@ -641,14 +641,24 @@ def run_served(args):
     """Poisson request stream through the request server (pa_server_*): requests
     are submitted at their arrival times from one thread, results are waited
     for and released in submission order from another; latency is the server's
-    own clock from submit to the control thread seeing the batch complete."""
+    own clock from submit to the control thread seeing the batch complete.
+    With N ranks, rank r serves the requests whose index is r mod N (a round-robin
+    router: one server per GPU, no collective on the data path); the job's value
+    is all ranks' edges over the slowest rank's span, and p50/p99 are over all
+    requests."""
     import queue
     import torch
+    import torch.distributed as dist
     import cuppa_b200 as pa
     from cuppa_b200.workloads import serve_requests
 
-    torch.cuda.set_device(0)
-    reqs = serve_requests(args.serve_seconds, args.rate)
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    all_reqs = serve_requests(args.serve_seconds, args.rate)
+    reqs = [r for i, r in enumerate(all_reqs) if i % world == rank]
     free_b, _ = torch.cuda.mem_get_info()
     budget = min(int(args.serve_budget_gb * 1e9), int(free_b * 0.9))
     prms = [pa.make_params(r["n"], r["d"], r["p"], seed=r["seed"], id_bits=32,
@@ -657,12 +667,14 @@ def run_served(args):
     lat, edges_done, statuses = [], 0, []
     outputs = {"pairs": pa.PA_OUT_PAIRS, "csr": pa.PA_OUT_CSR,
                "both": pa.PA_OUT_PAIRS | pa.PA_OUT_CSR}[args.serve_outputs]
-    with pa.Server(budget_bytes=budget, outputs=outputs) as srv, ClockSampler(0) as clk:
+    with pa.Server(budget_bytes=budget, outputs=outputs) as srv, ClockSampler(local) as clk:
         # warm-up: a few requests, waited for and released
         for q in prms[: args.warmup]:
             t = srv.submit(q)
             srv.wait(t)
             srv.release(t)
+        if world > 1:
+            dist.barrier()          # every rank starts the arrival clock together
         t0 = time.perf_counter()
 
         def submitter():
@@ -692,27 +704,42 @@ def run_served(args):
         th.join()
         st = srv.stats().as_dict()
     span_s = (last_done - first_submit) / 1e9
+    ok = all(x == 0 for x in statuses)
+    n_req = len(reqs)
+    if world > 1:
+        span_s = max_over_ranks(span_s, world, "cuda")
+        gathered = [None] * world
+        dist.all_gather_object(gathered, (lat, edges_done, ok, n_req))
+        lat = [x for g in gathered for x in g[0]]
+        edges_done = sum(g[1] for g in gathered)
+        ok = all(g[2] for g in gathered)
+        n_req = sum(g[3] for g in gathered)
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0 if ok else 1
     lat_sorted = sorted(lat)
 
     def pct(x):
         return lat_sorted[min(len(lat_sorted) - 1, int(round(x / 100 * (len(lat_sorted) - 1))))]
 
-    ok = all(x == 0 for x in statuses)
     line = {
         "metric": "served edges/s with p50/p99 latency (continuous batching)",
-        "value": edges_done / span_s, "unit": "edges/s", "n_gpus": 1, "steps": 1,
+        "value": edges_done / span_s, "unit": "edges/s", "n_gpus": world, "steps": 1,
         "warmup": args.warmup, "ms_per_step": span_s * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "scaling": "strong", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (generator parameters only)",
         "config": {"workload": f"Poisson {args.rate:g} req/s for {args.serve_seconds:g} s: "
                                "n=round(10^U(4,8)), d=U{2..16}, p=U(0.2,0.8), int32, clique seed",
-                   "requests": len(reqs), "budget_gb": budget / 1e9,
+                   "requests": n_req, "budget_gb_per_gpu": budget / 1e9,
+                   "parallelism": f"requests round-robin over {world} servers (one per rank)"
+                   if world > 1 else "single",
                    "output": {"pairs": "edge list (PAIRS)", "csr": "undirected CSR",
                               "both": "edge list and undirected CSR"}[args.serve_outputs]
                              + " kept on the device until released"},
         "p50_ms": pct(50), "p99_ms": pct(99), "max_ms": lat_sorted[-1],
-        "requests_per_s": len(reqs) / span_s, "all_ok": ok, "server_stats": st,
-        "statuses": {str(c): statuses.count(c) for c in sorted(set(statuses))},
+        "requests_per_s": n_req / span_s, "all_ok": ok, "server_stats_rank0": st,
+        "statuses_rank0": {str(c): statuses.count(c) for c in sorted(set(statuses))},
         "gpu_launches": st["batches"] * 2 + (st["completed"] * 11 if outputs & pa.PA_OUT_CSR else 0),
         "clocks": clk.summary(),
     }

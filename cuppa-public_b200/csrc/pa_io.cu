@@ -109,13 +109,13 @@ int pa_write_degree_distribution(const pa_params *prm, const void *d_edges, cons
     std::map<uint64_t, uint64_t> hub;
     for (unsigned long long k : big) ++hub[k];
     FILE *f = std::fopen(path, "wb");
-    if (!f) return PA_ERR_INVALID;
+    if (!f) return PA_ERR_IO;
     std::fprintf(f, "Degree,Count\n");
     for (uint64_t k = 1; k < kGlobalBins; ++k)
         if (h[k]) std::fprintf(f, "%llu,%llu\n", (unsigned long long)k, (unsigned long long)h[k]);
     for (const auto &kv : hub)
         std::fprintf(f, "%llu,%llu\n", (unsigned long long)kv.first, (unsigned long long)kv.second);
-    return std::fclose(f) == 0 ? PA_OK : PA_ERR_INVALID;
+    return std::fclose(f) == 0 ? PA_OK : PA_ERR_IO;
 }
 
 }  // extern "C"

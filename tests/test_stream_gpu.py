@@ -178,3 +178,18 @@ def test_runner_writes_slots_graph(cuda_ok, tmp_path):
     G = orc.generate(30000, 4, 0.5, 5, orc.SEED_STAR_REF)
     with open(out, "rb") as f:
         assert f.read() == text_of(orc.pairs_slot_order(G, orc.SEED_STAR_REF))
+
+
+def test_unwritable_paths_report_io_errors(pa, cuda_ok, tmp_path):
+    prm = pa.make_params(1000, 4, 0.5)
+    E, _ = pa.generate(prm)
+    bad = str(tmp_path / "no-such-dir" / "x.txt")
+    with pytest.raises(pa.CuppaError) as ei:
+        pa.write_edges(prm, E, bad)
+    assert ei.value.status == pa.PA_ERR_IO
+    with pytest.raises(pa.CuppaError) as ei:
+        pa.write_degree_distribution(prm, E, bad)
+    assert ei.value.status == pa.PA_ERR_IO
+    with pytest.raises(pa.CuppaError) as ei:
+        pa.generate_to_file(prm, bad)
+    assert ei.value.status == pa.PA_ERR_IO

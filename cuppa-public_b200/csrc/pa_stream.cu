@@ -640,6 +640,8 @@ int pa_generate_to_file(const pa_params *prm, const char *path, int format, pa_s
     int rc = make_plan(prm, &p);
     if (rc != PA_OK) return rc;
     if (!path || (format != PA_FORMAT_TEXT && format != PA_FORMAT_BINARY)) return PA_ERR_INVALID;
+    FILE *f = std::fopen(path, "wb");   // fail before generating, not after
+    if (!f) return PA_ERR_IO;
     void *edges = nullptr, *scratch = nullptr;
     cudaStream_t s = nullptr;
     cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
@@ -650,16 +652,9 @@ int pa_generate_to_file(const pa_params *prm, const char *path, int format, pa_s
         pa_stats st;
         if (rc == PA_OK) rc = pa_generate_finish(scratch, &st, s);
         if (rc == PA_OK && stats) *stats = st;
-        if (rc == PA_OK) {
-            FILE *f = std::fopen(path, "wb");
-            if (!f) {
-                rc = PA_ERR_IO;
-            } else {
-                rc = stream_edges(prm, p, edges, format, 0, file_sink, f, s, bytes_out);
-                if (std::fclose(f) != 0 && rc == PA_OK) rc = PA_ERR_IO;
-            }
-        }
+        if (rc == PA_OK) rc = stream_edges(prm, p, edges, format, 0, file_sink, f, s, bytes_out);
     }
+    if (std::fclose(f) != 0 && rc == PA_OK) rc = PA_ERR_IO;
     if (edges) cudaFree(edges);
     if (scratch) cudaFree(scratch);
     if (s) cudaStreamDestroy(s);

@@ -166,12 +166,62 @@ __global__ void __launch_bounds__(1024) tile_scan_kernel(unsigned long long *v, 
     if (threadIdx.x == 1023) *total = part[1023];
 }
 
+// The four 32-bit words starting s bytes (s < 16, a multiple-of-4 part ws = s/4
+// and a byte part) into the 32 bytes a:b.
+__device__ __forceinline__ uint4 shift_bytes(const uint4 &a, const uint4 &b, uint32_t ws,
+                                             uint32_t bits)
+{
+    uint32_t x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    uint4 r;
+    // ws is the same for the whole block: the branches do not diverge, and the
+    // constant indices keep x in registers
+    switch (ws) {
+    case 0:
+        r = make_uint4(__funnelshift_r(x[0], x[1], bits), __funnelshift_r(x[1], x[2], bits),
+                       __funnelshift_r(x[2], x[3], bits), __funnelshift_r(x[3], x[4], bits));
+        break;
+    case 1:
+        r = make_uint4(__funnelshift_r(x[1], x[2], bits), __funnelshift_r(x[2], x[3], bits),
+                       __funnelshift_r(x[3], x[4], bits), __funnelshift_r(x[4], x[5], bits));
+        break;
+    case 2:
+        r = make_uint4(__funnelshift_r(x[2], x[3], bits), __funnelshift_r(x[3], x[4], bits),
+                       __funnelshift_r(x[4], x[5], bits), __funnelshift_r(x[5], x[6], bits));
+        break;
+    default:
+        r = make_uint4(__funnelshift_r(x[3], x[4], bits), __funnelshift_r(x[4], x[5], bits),
+                       __funnelshift_r(x[5], x[6], bits), __funnelshift_r(x[6], x[7], bits));
+        break;
+    }
+    return r;
+}
+
+// Copy `len` bytes of the tile text to out (any alignment): the bytes up to the
+// first 16-byte boundary of out and after the last one go one by one, the rest
+// as aligned 16-byte stores, each assembled from two aligned 16-byte shared
+// loads (the shared buffer carries 32 bytes of slack past the text).
+__device__ __forceinline__ void copy_out(unsigned char *out, const unsigned char *s_text,
+                                         uint32_t len)
+{
+    uint32_t head = (uint32_t)((16u - (reinterpret_cast<uintptr_t>(out) & 15u)) & 15u);
+    if (head > len) head = len;
+    const uint32_t chunks = (len - head) / 16u;
+    const uint32_t tail0 = head + chunks * 16u;
+    if (threadIdx.x < head) out[threadIdx.x] = s_text[threadIdx.x];
+    if (threadIdx.x < len - tail0) out[tail0 + threadIdx.x] = s_text[tail0 + threadIdx.x];
+    const uint32_t ws = (head & 15u) >> 2, bits = (head & 3u) * 8u;
+    const uint4 *src = reinterpret_cast<const uint4 *>(s_text) + (head >> 4);
+    uint4 *dst = reinterpret_cast<uint4 *>(out + head);
+    for (uint32_t k = threadIdx.x; k < chunks; k += kFmtThreads)
+        dst[k] = shift_bytes(src[k], src[k + 1], ws, bits);
+}
+
 // Pass 2: each tile formats its lines into shared memory at their block-scanned
 // offsets, then copies the bytes to the chunk buffer at the tile's offset.
 template <typename Id, bool Slots>
 __global__ void __launch_bounds__(kFmtThreads) text_write_kernel(const FmtArgs f)
 {
-    extern __shared__ unsigned char s_text[];
+    extern __shared__ __align__(16) unsigned char s_text[];
     __shared__ uint32_t s_warp[kFmtThreads / 32];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     for (uint64_t t = blockIdx.x; t < f.n_tiles; t += gridDim.x) {
@@ -212,8 +262,7 @@ __global__ void __launch_bounds__(kFmtThreads) text_write_kernel(const FmtArgs f
             __syncthreads();
         }
         const unsigned long long o = f.tile_len[t];
-        unsigned char *out = f.out + o;
-        for (uint32_t i = threadIdx.x; i < base; i += kFmtThreads) out[i] = s_text[i];
+        copy_out(f.out + o, s_text, base);
         __syncthreads();
     }
 }
@@ -465,7 +514,7 @@ int stream_edges(const pa_params *prm, const GenPlan &p, const void *d_edges, in
     const uint32_t max_line = 2 * dec_digits(prm->n - 1) + 2;
     const uint64_t chunk_cap = text ? chunk_rows * d * max_line : chunk_rows * d * pair_bytes;
     const uint64_t tiles_cap = (chunk_rows + tile_rows - 1) / tile_rows;
-    const uint32_t smem = tile_rows * d * max_line;
+    const uint32_t smem = tile_rows * d * max_line + 32;   // + slack read by copy_out
     const bool direct = !text && !p.slots;   // PAIRS binary: copy the edge list itself
 
     Writer W;

@@ -430,6 +430,23 @@ __device__ __forceinline__ void map_unit(const LevelTables &tab, uint32_t count,
     t = __ldg(tab.loc_start + (uint64_t)l * count + inst) + (r - __ldg(ib + inst));
 }
 
+// map_unit, plus the segment that T falls in: the global units [lo, hi) of
+// (level, graph inst), whose unit lo is the graph's local unit t0.  Every T in
+// it maps to (inst, t0 + T - lo) without a search.
+__device__ __forceinline__ void map_unit_seg(const LevelTables &tab, uint32_t count,
+                                             unsigned long long T, uint32_t &inst,
+                                             unsigned long long &lo, unsigned long long &hi,
+                                             unsigned long long &t0)
+{
+    const uint32_t l = last_le(tab.lvl_base, tab.levels, T);
+    const unsigned long long base = __ldg(tab.lvl_base + l);
+    const unsigned long long *ib = tab.inst_base + (uint64_t)l * (count + 1);
+    inst = last_le(ib, count, T - base);
+    lo = base + __ldg(ib + inst);
+    hi = base + __ldg(ib + inst + 1);
+    t0 = __ldg(tab.loc_start + (uint64_t)l * count + inst);
+}
+
 // The start kernel's claim counters: warp w of a block claims from counter w,
 // which hands out start tiles w, w + 8, w + 16, ... (one atomic per tile, eight
 // addresses instead of one).

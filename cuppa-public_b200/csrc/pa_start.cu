@@ -200,8 +200,17 @@ template <typename Id, bool Slots>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) start_kernel(const StartArgs b)
 {
     __shared__ GenArgs s_args[kThreads / 32];
+    // per warp: the (level, graph) segment of its last claim, [lo, hi) and the
+    // local unit of lo -- a warp's claims T, T + 8, ... mostly stay inside one,
+    // and the two searches of map_unit cost as much as a tile's own work
+    __shared__ unsigned long long s_seg[kThreads / 32][3];
     const uint32_t warp = threadIdx.x >> 5;
     GenArgs &a = s_args[warp];
+    if ((threadIdx.x & 31u) == 0) {
+        s_seg[warp][0] = 1;   // empty segment
+        s_seg[warp][1] = 0;
+    }
+    __syncwarp();
 
     Lane L;
     L.lane = threadIdx.x & 31u;
@@ -250,7 +259,24 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) start_kernel(const Start
         if (T >= b.t_end) break;
         uint32_t i = 0;
         uint64_t t = T;
-        if (b.count != 1) map_unit(b.tab, b.count, T, i, t);
+        if (b.count != 1) {
+            const unsigned long long lo = s_seg[warp][0], hi = s_seg[warp][1];
+            if (T >= lo && T < hi) {
+                i = cur;   // the segment's graph is the one loaded
+                t = s_seg[warp][2] + (T - lo);
+            } else {
+                unsigned long long nlo, nhi, t0;
+                map_unit_seg(b.tab, b.count, T, i, nlo, nhi, t0);
+                t = t0 + (T - nlo);
+                __syncwarp();
+                if (L.lane == 0) {
+                    s_seg[warp][0] = nlo;
+                    s_seg[warp][1] = nhi;
+                    s_seg[warp][2] = t0;
+                }
+                __syncwarp();
+            }
+        }
         if (i != cur) {
             __syncwarp();
             const uint32_t *src = reinterpret_cast<const uint32_t *>(b.inst + i);

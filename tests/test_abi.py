@@ -163,3 +163,11 @@ def test_stream_edges_rejects_bad_arguments(pa):
                              ctypes.byref(total)) == pa.PA_ERR_INVALID
     assert L.pa_stream_edges(ctypes.byref(prm), ctypes.c_void_p(16), 0, 0, None, None, None,
                              ctypes.byref(total)) == pa.PA_ERR_INVALID
+
+
+def test_binding_fails_loudly_without_the_library(pa, monkeypatch, tmp_path):
+    """No silent fallback: a missing native library is an error, not a CPU path."""
+    monkeypatch.setattr(pa, "LIB_PATH", str(tmp_path / "libcuppa_pa.so"))
+    monkeypatch.setattr(pa, "_lib", None)
+    with pytest.raises(FileNotFoundError):
+        pa.lib()

@@ -65,3 +65,25 @@ def test_router_csr_outputs(pa, cuda_ok):
         want_rp, want_col = pa.build_csr(q, E)
         assert torch.equal(rowptr, want_rp) and torch.equal(col, want_col)
         r.release(t)
+
+
+def test_router_forgets_expired_results(pa, cuda_ok):
+    """A result dropped by its server's TTL stops counting against that server:
+    after the expiry the next equal request goes back to server 0."""
+    import time
+    with pa.Router([0, 0], budget_bytes=1 << 30, ttl_ns=50_000_000) as r:
+        q = pa.make_params(50_000, 4, 0.5, seed=11)
+        t0 = r.submit(q)
+        assert r.server_of(t0) == 0
+        rc, _ = r.wait(t0, 60_000_000_000)
+        assert rc == 0
+        t1 = r.submit(q)                       # server 0 still holds t0's bytes
+        assert r.server_of(t1) == 1
+        assert r.wait(t1, 60_000_000_000)[0] == 0
+        assert r.release(t1) == 0
+        time.sleep(0.3)                        # past the TTL: t0 expires unreleased
+        assert r.poll(t0)[0] == pa.PA_ERR_NOT_FOUND
+        t2 = r.submit(q)
+        assert r.server_of(t2) == 0
+        assert r.wait(t2, 60_000_000_000)[0] == 0
+        r.release(t2)

@@ -361,6 +361,7 @@ def run_gpu(args, w):
         else:
             kernel, k_edges, kern_s = "start_kernel", start_edges, statistics.mean(start_ms) / 1e3
         achieved = k_edges * bpe / kern_s / 1e9
+        traffic = load_traffic(args.workload)     # ncu DRAM bytes of one such launch
         launches = (1 if u_split > w["d"] + 1 else 0) + (1 if gen_edges > 0 else 0)
         line = {
             "metric": w.get("metric", METRIC), "value": value, "unit": "edges/s", "n_gpus": world,
@@ -374,7 +375,11 @@ def run_gpu(args, w):
                              "no flush needed"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
-                         "bytes_per_edge": bpe, "traffic": load_traffic(args.workload),
+                         "bytes_per_edge": bpe, "traffic": traffic,
+                         # the DRAM the launch actually moves (whole 128-byte lines
+                         # for random reads) over its measured time
+                         "traffic_gbs": traffic / kern_s / 1e9 if traffic else None,
+                         "traffic_frac": traffic / kern_s / 1e9 / peak if traffic else None,
                          "kernel": kernel, "launch_ms_mean": kern_s * 1e3,
                          "kernel_edges": k_edges},
             "phases_ms_mean": {"clear+fill (memsets)": statistics.mean(fill_ms),

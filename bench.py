@@ -182,23 +182,62 @@ def dist_setup():
     return world, rank, local
 
 
+def baseline_core() -> int:
+    """The host core the sequential baselines are pinned to (the first one this
+    process may use)."""
+    try:
+        return min(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return 0
+
+
+def pinned(fn, *a, **kw):
+    """Run fn on one core (Linux affinity of the calling thread), then restore."""
+    try:
+        old = os.sched_getaffinity(0)
+        os.sched_setaffinity(0, {baseline_core()})
+    except (AttributeError, OSError):
+        return fn(*a, **kw)
+    try:
+        return fn(*a, **kw)
+    finally:
+        os.sched_setaffinity(0, old)
+
+
+def pin_child():
+    """preexec_fn for the reference binaries: one core."""
+    try:
+        os.sched_setaffinity(0, {baseline_core()})
+    except (AttributeError, OSError):
+        pass
+
+
+def host_cores() -> int:
+    return os.cpu_count() or 0
+
+
 def cpu_baseline_oracle(w, nodes: int):
-    """The sequential oracle (1 core) on `nodes` nodes of the same (d, p, seed)."""
+    """The sequential oracle, pinned to one core, on `nodes` nodes of the same
+    (d, p, seed)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import _oracle as orc
     n = min(nodes, w["n"])
-    t0 = time.perf_counter()
-    if w.get("model", COPY) == BA:
-        orc.generate_ba(n, w["d"], w["seed"])
-        what = "Philox restatement of SerialBA.cpp"
-    else:
-        orc.generate(n, w["d"], w["p"], w["seed"], w["seed_mode"])
-        what = "Philox restatement of SerialCopyModel3.cpp"
-    dt = time.perf_counter() - t0
+
+    def run():
+        t0 = time.perf_counter()
+        if w.get("model", COPY) == BA:
+            orc.generate_ba(n, w["d"], w["seed"])
+        else:
+            orc.generate(n, w["d"], w["p"], w["seed"], w["seed_mode"])
+        return time.perf_counter() - t0
+    what = ("Philox restatement of SerialBA.cpp" if w.get("model", COPY) == BA
+            else "Philox restatement of SerialCopyModel3.cpp")
+    dt = pinned(run)
     edges = orc.edge_count(n, w["d"], w["seed_mode"])
     return {"value": edges / dt, "unit": "edges/s", "cores": 1, "kind": "port",
+            "host_cores": host_cores(), "pinned_core": baseline_core(),
             "sample": f"oracle ({what}), n={n}, d={w['d']}, "
-                      f"p={w['p']}, {edges} edges in {dt:.2f} s, one thread"}
+                      f"p={w['p']}, {edges} edges in {dt:.2f} s, one thread on one core"}
 
 
 def run_reference(args, w):
@@ -225,6 +264,7 @@ def run_reference(args, w):
         with tempfile.TemporaryDirectory() as td:
             for i in range(args.warmup + args.steps):
                 out = subprocess.run([td if a == "{td}" else a for a in cmd], cwd=td,
+                                     preexec_fn=pin_child,
                                      capture_output=True, text=True, check=True).stdout
                 t = [float(x.split(":")[1]) for x in out.splitlines()
                      if x.startswith("Computation Time")][0]
@@ -236,14 +276,17 @@ def run_reference(args, w):
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import _oracle as orc
         edges = orc.edge_count(n, d, w["seed_mode"])
-        for i in range(args.warmup + args.steps):
+        def one():
             t0 = time.perf_counter()
             if ba:
                 orc.generate_ba(n, d, w["seed"])
             else:
                 orc.generate(n, d, w["p"], w["seed"], w["seed_mode"])
+            return time.perf_counter() - t0
+        for i in range(args.warmup + args.steps):
+            dt = pinned(one)
             if i >= args.warmup:
-                times.append(time.perf_counter() - t0)
+                times.append(dt)
     total = sum(times)
     value = edges * len(times) / total
     line = {
@@ -254,6 +297,7 @@ def run_reference(args, w):
         "data": "synthetic (generator parameters only)",
         "config": {"workload": w["name"], "sample_nodes": n},
         "cpu_baseline": {"value": value, "unit": "edges/s", "cores": 1, "kind": kind,
+                         "host_cores": host_cores(), "pinned_core": baseline_core(),
                          "sample": sample},
         "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -516,15 +560,17 @@ def reference_writer_sample(n, d, p):
     if not (os.path.exists(scm) and os.path.exists(wr)):
         return None
     with tempfile.TemporaryDirectory() as td:
-        out = subprocess.run([scm, str(n), str(d), str(p), td, "-"], cwd=td,
+        out = subprocess.run([scm, str(n), str(d), str(p), td, "-"], cwd=td, preexec_fn=pin_child,
                              capture_output=True, text=True, check=True).stdout
         t_gen = [float(x.split(":")[1]) for x in out.splitlines()
                  if x.startswith("Computation Time")][0]
-        out = subprocess.run([wr, str(n), str(d), str(p), "/dev/null"], capture_output=True,
+        out = subprocess.run([wr, str(n), str(d), str(p), "/dev/null"], preexec_fn=pin_child,
+                             capture_output=True,
                              text=True, check=True).stdout
         t_wr = [float(x.split(":")[1]) for x in out.splitlines() if x.startswith("Write Time")][0]
     edges = (n - d) * d
     return {"value": edges / (t_gen + t_wr), "unit": "edges/s", "cores": 1, "kind": "reference",
+            "host_cores": host_cores(), "pinned_core": baseline_core(),
             "sample": f"reference -A scm generation ({t_gen:.2f} s) + PAHelper::writeGraphToDisk "
                       f"to /dev/null ({t_wr:.2f} s), n={n}, d={d}, p={p}, int32, one thread"}
 

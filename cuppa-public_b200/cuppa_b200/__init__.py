@@ -581,6 +581,38 @@ class cuPPA:  # noqa: N801 - reference class name
             return f.read()
 
 
+class SerialCopyModel:  # noqa: N801 - reference class name
+    """SerialCopyModel(nNodes, mEdgesPerNode, p) -- src/PA/SPA/SerialCopyModel.h,
+    the sequential copy model of -A scm (src/main.cu:93-98, SerialCopyModel.h:26-45),
+    run on the device:
+    the same model as cuPPA on the reference's star seed graph
+    (SerialCopyModel3.cpp:38-49).  generateGraph keeps the edges; the degree
+    distribution is the "Degree,Count" CSV of src/PA/SPA/PAHelper.hpp:15-67."""
+
+    def __init__(self, nNodes: int, mEdgesPerNode: int, p: float):
+        self._N, self._M, self._p = int(nNodes), int(mEdgesPerNode), float(p)
+        self.edges = None
+        self.stats: Optional[PaStats] = None
+        self._prm: Optional[PaParams] = None
+
+    def generateGraph(self, conf: ExperimentConfiguration):
+        self._N, self._M, self._p = int(conf._n1), int(conf._x1), float(conf._alpha)
+        self._prm = make_params(self._N, self._M, self._p, seed=conf.seed, id_bits=conf.id_bits,
+                                seed_mode=PA_SEED_STAR_REF, blocks=conf._blockSize)
+        self.edges, self.stats = generate(self._prm)
+        if conf._FLAG_SHOW_DEGREE_DISTRIBUTION:
+            self.printDegreeDistribution(conf)
+        return self.edges
+
+    def printDegreeDistribution(self, conf: ExperimentConfiguration) -> str:
+        if self.edges is None:
+            raise RuntimeError("generateGraph first")
+        path = os.path.join(conf._outputDir, conf._distfile1)
+        write_degree_distribution(self._prm, self.edges, path)
+        with open(path) as f:
+            return f.read()
+
+
 class SerialBA:  # noqa: N801 - reference class name
     """SerialBA(nNodes, mEdgesPerNode) -- src/PA/SPA/SerialBA.h:17-37, the
     repeated-nodes Barabasi-Albert generator of -A sba, run on the device

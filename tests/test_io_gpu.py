@@ -67,3 +67,17 @@ def test_cuppa_class_mirror(pa, cuda_ok, tmp_path):
     with open(os.path.join(str(tmp_path), "dd.csv")) as f:
         assert f.read() == orc.dd_csv_from_degrees(orc.degrees(G, orc.SEED_CLIQUE))
     assert (g.generateGraphAdaptive(conf) == edges).all()
+
+
+def test_serial_copy_model_mirror(pa, cuda_ok, tmp_path):
+    """SerialCopyModel(n, m, p).generateGraph(conf), the reference's -A scm entry:
+    the copy model on the reference's star seed."""
+    conf = pa.ExperimentConfiguration(_algorithm="scm", _n1=50000, _x1=4, _alpha=0.3,
+                                      _FLAG_SHOW_DEGREE_DISTRIBUTION=True, _distfile1="dd.csv",
+                                      _outputDir=str(tmp_path), seed=13)
+    g = pa.SerialCopyModel(conf._n1, conf._x1, conf._alpha)
+    edges = g.generateGraph(conf)
+    G = orc.generate(50000, 4, 0.3, 13, orc.SEED_STAR_REF)
+    assert (edges.cpu().numpy().astype(np.int64) == orc.pairs_slot_order(G, orc.SEED_STAR_REF)).all()
+    with open(os.path.join(str(tmp_path), "dd.csv")) as f:
+        assert f.read() == orc.dd_csv_from_degrees(orc.degrees(G, orc.SEED_STAR_REF))

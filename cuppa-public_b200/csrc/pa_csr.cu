@@ -270,9 +270,10 @@ __global__ void __launch_bounds__(kRadixThreads) radix_hist_kernel(const void *s
 template <uint32_t NB>
 struct RadixSmem {
     unsigned long long stage[kRadixTile];
-    unsigned long long goff[NB];                  // this tile's global offset per digit
-    uint16_t wcnt[kRadixWarps][NB];               // per-warp digit counts, then bases (<= tile)
-    uint32_t lstart[NB];                          // digit start within the tile
+    unsigned long long goff[NB];                  // global offset of the digit's run, less its
+                                                  // start within the tile
+    uint16_t wcnt[kRadixWarps][NB];               // per-warp digit counts, then the warp's base
+                                                  // within the tile (digit start included)
     uint16_t lrank[kRadixTile];                   // rank within the warp's items of its digit
 };
 
@@ -326,7 +327,10 @@ __global__ void __launch_bounds__(kRadixThreads, 2) radix_scatter_kernel(const v
     }
     __syncthreads();
     // 2. per digit (thread j owns digits j*PER .. j*PER+PER-1): warp bases in
-    // warp order, the digit's total, then the digits' starts within the tile
+    // warp order, the digit's total, then the digits' starts within the tile,
+    // folded into the warp bases and the global offsets so that phases 3 and 4
+    // make one randomly indexed shared access each per item (shared memory, not
+    // DRAM, is what bounds this kernel)
     uint32_t tot[PER];
     uint32_t mine = 0;
 #pragma unroll
@@ -359,7 +363,11 @@ __global__ void __launch_bounds__(kRadixThreads, 2) radix_scatter_kernel(const v
 #pragma unroll
     for (uint32_t q = 0; q < PER; ++q) {
         const uint32_t dg = threadIdx.x * PER + q;
-        if (dg < NB) S.lstart[dg] = run;
+        if (dg < NB) {
+            for (uint32_t w = 0; w < kRadixWarps; ++w)   // <= tile size: fits 16 bits
+                S.wcnt[w][dg] = (uint16_t)(S.wcnt[w][dg] + run);
+            S.goff[dg] -= run;    // the run's global start >= its start in the tile
+        }
         run += tot[q];
     }
     __syncthreads();
@@ -376,7 +384,7 @@ __global__ void __launch_bounds__(kRadixThreads, 2) radix_scatter_kernel(const v
             const uint32_t k = wo + (r0 + q) * 32 + lane;
             if (k < tcount) {
                 const uint32_t dg = (uint32_t)(its[q] >> (32 + shift)) & MASK;
-                S.stage[S.lstart[dg] + S.wcnt[warp][dg] + S.lrank[k]] = its[q];
+                S.stage[S.wcnt[warp][dg] + S.lrank[k]] = its[q];
             }
         }
     }
@@ -385,7 +393,7 @@ __global__ void __launch_bounds__(kRadixThreads, 2) radix_scatter_kernel(const v
     for (uint32_t k = threadIdx.x; k < tcount; k += kRadixThreads) {
         const unsigned long long it = S.stage[k];
         const uint32_t dg = (uint32_t)(it >> (32 + shift)) & MASK;
-        dst[S.goff[dg] + (k - S.lstart[dg])] = it;
+        dst[S.goff[dg] + k] = it;
     }
 }
 

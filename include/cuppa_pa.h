@@ -350,6 +350,9 @@ int pa_router_device_of(pa_router *r, uint64_t ticket, int32_t *device);
 /* Statistics of server `index` (0..size-1), or summed over all with index == size. */
 int pa_router_stats_get(pa_router *r, uint32_t index, pa_server_stats *out);
 uint32_t pa_router_size(const pa_router *r);
+/* Destroys every server (each as pa_server_destroy) and the router; no thread may
+ * be inside a pa_router_* call on this handle.  Submit, poll, wait and release
+ * may be called from any threads concurrently. */
 int pa_router_destroy(pa_router *r);
 /* The placement rule alone (host arithmetic): the index i minimising
  * (load_bytes[i] + request_bytes) / budget_bytes[i], exactly; ties go to the

@@ -323,6 +323,9 @@ __global__ void __launch_bounds__(kRadixThreads, 2) radix_scatter_kernel(const v
             }
             old = __shfl_sync(kFull, old, leader);
             if (valid) S.lrank[k] = (uint16_t)(old + __popc(peers & lt));
+            // the next round's leader for a digit may be another lane: order
+            // this round's counter stores before the next round's loads
+            __syncwarp();
         }
     }
     __syncthreads();

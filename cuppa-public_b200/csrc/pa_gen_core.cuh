@@ -15,6 +15,10 @@ namespace gen {
 constexpr uint32_t kFull = 0xffffffffu;
 constexpr uint32_t kThreads = 256;
 constexpr uint32_t kMinBlocks = 4;   // 32 resident warps per SM: at most 64 registers
+// The start kernel: 40 warps per SM (at most 51 registers; a few bytes spill).
+// More warps put more copy reads in flight: C3 69.4 -> 68.2 ms at p = 0.5 and
+// 278 -> 270 ms at p = 0, where the retry tails of a tile leave lanes idle.
+constexpr uint32_t kStartMinBlocks = 5;
 
 enum : uint32_t { ST_KNOWN = 0, ST_PEND_GLOBAL = 1, ST_PEND_TILE = 2 };
 

@@ -197,7 +197,7 @@ __device__ __forceinline__ void set_lane(Lane &L, const GenArgs &a)
 }
 
 template <typename Id, bool Slots>
-__global__ void __launch_bounds__(kThreads, kMinBlocks) start_kernel(const StartArgs b)
+__global__ void __launch_bounds__(kThreads, kStartMinBlocks) start_kernel(const StartArgs b)
 {
     __shared__ GenArgs s_args[kThreads / 32];
     // per warp: the (level, graph) segment of its last claim, [lo, hi) and the

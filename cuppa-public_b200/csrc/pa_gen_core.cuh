@@ -16,9 +16,11 @@ constexpr uint32_t kFull = 0xffffffffu;
 constexpr uint32_t kThreads = 256;
 constexpr uint32_t kMinBlocks = 4;   // 32 resident warps per SM: at most 64 registers
 // The start kernel: 40 warps per SM (at most 51 registers; a few bytes spill).
-// More warps put more copy reads in flight: C3 69.4 -> 68.2 ms at p = 0.5 and
-// 278 -> 270 ms at p = 0, where the retry tails of a tile leave lanes idle.
+// More warps put more copy reads in flight: C3 69.4 -> 68.2 ms at p = 0.5.
 constexpr uint32_t kStartMinBlocks = 5;
+// p = 0 (every slot a copy, several retries per node): 48 warps per SM pay off
+// there (C3 270 -> 259 ms) though they cost at p = 0.5 (68.1 -> 71.7 ms).
+constexpr uint32_t kStartMinBlocksCopy = 6;
 
 enum : uint32_t { ST_KNOWN = 0, ST_PEND_GLOBAL = 1, ST_PEND_TILE = 2 };
 
@@ -471,8 +473,9 @@ struct StartArgs {
 
 // Launch the start kernel; `blocks` 0 = one wave.  The claim counters must be
 // zero and every pair of the graphs' start regions all-ones (fill_start).
+// copy_only: a copy-model graph with p = 0, launched at kStartMinBlocksCopy.
 int launch_start(uint32_t id_bytes, const StartArgs &b, uint32_t blocks, cudaStream_t s,
-                 bool slots = false);
+                 bool slots = false, bool copy_only = false);
 
 // Set every byte of the pairs of nodes [u_first, start_end) of each of `count`
 // graphs to 0xff (one launch).

@@ -196,8 +196,8 @@ __device__ __forceinline__ void set_lane(Lane &L, const GenArgs &a)
     L.gmask = L.used ? (a.d == 32 ? kFull : (((1u << a.d) - 1u) << (L.g * a.d))) : 0u;
 }
 
-template <typename Id, bool Slots>
-__global__ void __launch_bounds__(kThreads, kStartMinBlocks) start_kernel(const StartArgs b)
+template <typename Id, bool Slots, uint32_t MinBlocks>
+__global__ void __launch_bounds__(kThreads, MinBlocks) start_kernel(const StartArgs b)
 {
     __shared__ GenArgs s_args[kThreads / 32];
     // per warp: the (level, graph) segment of its last claim, [lo, hi) and the
@@ -347,10 +347,10 @@ __global__ void fill_start_kernel(const GenArgs *inst, uint32_t y0, uint32_t id_
         p[x] = ones;
 }
 
-template <typename Id, bool Slots>
+template <typename Id, bool Slots, uint32_t MinBlocks>
 int launch_start_t(const StartArgs &b, uint32_t blocks, cudaStream_t s)
 {
-    auto kern = start_kernel<Id, Slots>;
+    auto kern = start_kernel<Id, Slots, MinBlocks>;
     if (blocks == 0) {
         int dev = 0, sms = 0, per_sm = 0;
         cudaError_t e = cudaGetDevice(&dev);
@@ -371,14 +371,22 @@ int launch_start_t(const StartArgs &b, uint32_t blocks, cudaStream_t s)
 
 }  // namespace
 
-int launch_start(uint32_t id_bytes, const StartArgs &b, uint32_t blocks, cudaStream_t s,
-                 bool slots)
+template <uint32_t MinBlocks>
+int launch_start_m(uint32_t id_bytes, const StartArgs &b, uint32_t blocks, cudaStream_t s,
+                   bool slots)
 {
     if (slots)
-        return id_bytes == 8 ? launch_start_t<int64_t, true>(b, blocks, s)
-                             : launch_start_t<int32_t, true>(b, blocks, s);
-    return id_bytes == 8 ? launch_start_t<int64_t, false>(b, blocks, s)
-                         : launch_start_t<int32_t, false>(b, blocks, s);
+        return id_bytes == 8 ? launch_start_t<int64_t, true, MinBlocks>(b, blocks, s)
+                             : launch_start_t<int32_t, true, MinBlocks>(b, blocks, s);
+    return id_bytes == 8 ? launch_start_t<int64_t, false, MinBlocks>(b, blocks, s)
+                         : launch_start_t<int32_t, false, MinBlocks>(b, blocks, s);
+}
+
+int launch_start(uint32_t id_bytes, const StartArgs &b, uint32_t blocks, cudaStream_t s,
+                 bool slots, bool copy_only)
+{
+    return copy_only ? launch_start_m<kStartMinBlocksCopy>(id_bytes, b, blocks, s, slots)
+                     : launch_start_m<kStartMinBlocks>(id_bytes, b, blocks, s, slots);
 }
 
 int fill_start(uint32_t id_bytes, const GenArgs *d_inst, uint32_t count, uint64_t max_pairs,

@@ -21,6 +21,18 @@ constexpr uint32_t kStartMinBlocks = 5;
 // p = 0 (every slot a copy, several retries per node): 48 warps per SM pay off
 // there (C3 270 -> 259 ms) though they cost at p = 0.5 (68.1 -> 71.7 ms).
 constexpr uint32_t kStartMinBlocksCopy = 6;
+// A single graph with a small start region is bound by its dependency chains'
+// latency, which the spills of the wider variants lengthen: four blocks, 64
+// registers, no spills.
+constexpr uint32_t kStartMinBlocksSmall = 4;
+constexpr uint64_t kStartLargeNodes = 1ull << 24;
+
+// The start-kernel variant for one graph: start region nodes, copy-only (p = 0).
+inline uint32_t start_min_blocks(uint64_t start_nodes, bool copy_only)
+{
+    if (start_nodes < kStartLargeNodes) return kStartMinBlocksSmall;
+    return copy_only ? kStartMinBlocksCopy : kStartMinBlocks;
+}
 
 enum : uint32_t { ST_KNOWN = 0, ST_PEND_GLOBAL = 1, ST_PEND_TILE = 2 };
 
@@ -473,9 +485,9 @@ struct StartArgs {
 
 // Launch the start kernel; `blocks` 0 = one wave.  The claim counters must be
 // zero and every pair of the graphs' start regions all-ones (fill_start).
-// copy_only: a copy-model graph with p = 0, launched at kStartMinBlocksCopy.
+// min_blocks: the variant's resident blocks per SM (start_min_blocks picks it).
 int launch_start(uint32_t id_bytes, const StartArgs &b, uint32_t blocks, cudaStream_t s,
-                 bool slots = false, bool copy_only = false);
+                 bool slots = false, uint32_t min_blocks = kStartMinBlocks);
 
 // Set every byte of the pairs of nodes [u_first, start_end) of each of `count`
 // graphs to 0xff (one launch).

@@ -433,8 +433,9 @@ int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, vo
         sa.ctl = a.ctl;
         mrc = mark(1);
         if (mrc != PA_OK) return mrc;
-        const int rc = launch_start(plan.id_bytes, sa, blocks, stream, plan.slots,
-                                    plan.pth == 0 && plan.model == PA_MODEL_COPY);
+        const int rc = launch_start(
+            plan.id_bytes, sa, blocks, stream, plan.slots,
+            start_min_blocks(plan.u_split - plan.u_first, plan.pth == 0 && plan.model == PA_MODEL_COPY));
         if (rc != PA_OK) return rc;
         if (plan.u_split >= prm->n) {
             mrc = mark(2);

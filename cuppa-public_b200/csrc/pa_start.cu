@@ -383,10 +383,13 @@ int launch_start_m(uint32_t id_bytes, const StartArgs &b, uint32_t blocks, cudaS
 }
 
 int launch_start(uint32_t id_bytes, const StartArgs &b, uint32_t blocks, cudaStream_t s,
-                 bool slots, bool copy_only)
+                 bool slots, uint32_t min_blocks)
 {
-    return copy_only ? launch_start_m<kStartMinBlocksCopy>(id_bytes, b, blocks, s, slots)
-                     : launch_start_m<kStartMinBlocks>(id_bytes, b, blocks, s, slots);
+    if (min_blocks == kStartMinBlocksCopy)
+        return launch_start_m<kStartMinBlocksCopy>(id_bytes, b, blocks, s, slots);
+    if (min_blocks == kStartMinBlocksSmall)
+        return launch_start_m<kStartMinBlocksSmall>(id_bytes, b, blocks, s, slots);
+    return launch_start_m<kStartMinBlocks>(id_bytes, b, blocks, s, slots);
 }
 
 int fill_start(uint32_t id_bytes, const GenArgs *d_inst, uint32_t count, uint64_t max_pairs,

@@ -22,10 +22,16 @@
 //    overlaps (different streams, or different host threads) race on it and
 //    produce undefined results; issue them on one stream or serialize them;
 //  * the device address of the array is looked up with cudaGetSymbolAddress
-//    on the first call on each device (with that device current) and cached.
+//    on the first call in each CUDA context (with that context's device
+//    current) and cached under the context's ID.  A context created anew --
+//    after cudaDeviceReset, or after the primary context was released and
+//    retained again -- has a new ID, so its first call looks the address up
+//    again instead of reusing one from a context that no longer exists.
 //    Make that first call before any stream capture begins;
 //  * each call clears the part of the array it uses before launching, so the
 //    contents a previous call left behind never leak into the result.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "pa_internal.h"
@@ -41,9 +47,44 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[PA_NOALLOC_SCRA
 
 constexpr int kMaxDevices = 128;
 std::mutex g_mu;
+unsigned long long g_ctx_id[kMaxDevices] = {};   // context the cached address belongs to
 void *g_addr[kMaxDevices] = {};
 
-// Device address of g_noalloc_scratch on the current device (set-up on first use).
+// Driver entry points for the context identity, fetched through the runtime so
+// the library needs no link against libcuda.
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+
+// ID of the calling thread's current CUDA context, 0 when none is current.
+// Context IDs are unique for the life of the process, unlike context handles,
+// which the driver may hand out again after a context is destroyed.
+int current_context_id(unsigned long long *id)
+{
+    *id = 0;
+    if (!g_ctx_get_current || !g_ctx_get_id) {
+        void *f0 = nullptr, *f1 = nullptr;
+        cudaDriverEntryPointQueryResult q0, q1;
+        cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0);
+        if (e != cudaSuccess) return set_cuda_error(e);
+        e = cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1);
+        if (e != cudaSuccess) return set_cuda_error(e);
+        if (q0 != cudaDriverEntryPointSuccess || q1 != cudaDriverEntryPointSuccess || !f0 || !f1)
+            return PA_ERR_NOT_SUPPORTED;
+        g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f0);
+        g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f1);
+    }
+    CUcontext ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS) return PA_ERR_CUDA;
+    if (!ctx) return PA_OK;
+    if (g_ctx_get_id(ctx, id) != CUDA_SUCCESS) return PA_ERR_CUDA;
+    return PA_OK;
+}
+
+// Device address of g_noalloc_scratch in the current context: looked up with
+// cudaGetSymbolAddress on the first call in each context and cached under the
+// context's ID.
 int noalloc_scratch(void **out)
 {
     int dev = 0;
@@ -51,10 +92,17 @@ int noalloc_scratch(void **out)
     if (e != cudaSuccess) return set_cuda_error(e);
     if (dev < 0 || dev >= kMaxDevices) return PA_ERR_NOT_SUPPORTED;
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_addr[dev]) {
+    unsigned long long ctx = 0;
+    int st = current_context_id(&ctx);
+    if (st != PA_OK) return st;
+    if (ctx == 0 || ctx != g_ctx_id[dev] || !g_addr[dev]) {
         void *p = nullptr;
+        // The lookup makes the device's primary context current if none was.
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return set_cuda_error(e);
+        st = current_context_id(&ctx);
+        if (st != PA_OK) return st;
+        g_ctx_id[dev] = ctx;
         g_addr[dev] = p;
     }
     *out = g_addr[dev];

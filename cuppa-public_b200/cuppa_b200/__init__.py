@@ -544,7 +544,7 @@ class cuPPA:  # noqa: N801 - reference class name
 
     Unlike the reference, the generated graph is kept (``self.edges``, a device
     tensor of (u, v) pairs) instead of being freed before return
-    (src/PA/cuPPA/cuPPA_1.cu:519-522)."""
+    (src/PA/cuPPA/cuPPA_1.cu:247-250)."""
 
     def __init__(self, nNodes: int, mEdgesPerNode: int, p: float):
         self._N, self._M, self._p = int(nNodes), int(mEdgesPerNode), float(p)

@@ -163,9 +163,10 @@ int pa_generate_finish(const void *d_scratch, pa_stats *out, void *stream);
  * the process exits; the caller passes only the parameters and the edge
  * buffer.  Requests whose scratch exceeds the array (roughly n > 65 million
  * nodes at d = 4, n > 8 million at d = 32) return PA_ERR_CAPACITY before any GPU
- * work.  The first call on a device looks the array's address up with
- * cudaGetSymbolAddress (with that device current) and caches it: make that
- * first call before any stream capture begins.  All calls on a device share the
+ * work.  The first call in a CUDA context looks the array's address up with
+ * cudaGetSymbolAddress (with that context's device current) and caches it under
+ * the context's ID, so a context created anew after cudaDeviceReset is looked
+ * up again: make that first call before any stream capture begins.  All calls on a device share the
  * array, so calls whose GPU work overlaps race on it: issue them on one stream
  * or serialize them.  Each call clears what it uses, generates on `stream`,
  * waits for it, fills *stats (may be NULL) and returns the device status. */

@@ -108,6 +108,75 @@ __global__ void degree_slots_kernel(const Id *S, uint64_t rows, uint32_t d, uint
     }
 }
 
+// MurmurHash3's 64-bit finalizer (Appleby, public domain): a bijective mix.
+__device__ __forceinline__ uint64_t fmix64(uint64_t k)
+{
+    k ^= k >> 33;
+    k *= 0xFF51AFD7ED558CCDull;
+    k ^= k >> 33;
+    k *= 0xC4CEB9FE1A85EC53ull;
+    k ^= k >> 33;
+    return k;
+}
+
+// Digest term of id x at position pos (the position is mixed in first, so two
+// elements that trade places change the digest).
+__device__ __forceinline__ uint64_t digest_term(uint64_t pos, uint64_t x)
+{
+    return fmix64(fmix64(pos * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull) ^ x);
+}
+
+// Sum and xor of the digest terms of x[0..count), positions from `base`.  A
+// thread takes 16-byte vectors (two int64 or four int32 ids) with streaming
+// loads when x is 16-byte aligned; a warp and then the block reduce, and one
+// thread per block adds to acc (sum) and xors into acc + 1.
+template <typename Id>
+__global__ void __launch_bounds__(256) digest_kernel(const Id *x, uint64_t count, uint64_t base,
+                                                     bool vec, unsigned long long *acc)
+{
+    constexpr uint32_t V = 16 / sizeof(Id);
+    uint64_t sum = 0, xr = 0;
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t nvec = vec ? count / V : 0;
+    const uint4 *xv = reinterpret_cast<const uint4 *>(x);
+    for (uint64_t i = tid; i < nvec; i += stride) {
+        const uint4 w = __ldcs(xv + i);
+        Id vals[V];
+        memcpy(vals, &w, sizeof(w));
+#pragma unroll
+        for (uint32_t j = 0; j < V; ++j) {
+            const uint64_t h = digest_term(base + i * V + j, (uint64_t)(int64_t)vals[j]);
+            sum += h;
+            xr ^= h;
+        }
+    }
+    for (uint64_t i = nvec * V + tid; i < count; i += stride) {
+        const uint64_t h = digest_term(base + i, (uint64_t)(int64_t)x[i]);
+        sum += h;
+        xr ^= h;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        sum += __shfl_xor_sync(kFull, sum, off);
+        xr ^= __shfl_xor_sync(kFull, xr, off);
+    }
+    __shared__ uint64_t ssum[8], sxr[8];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        ssum[warp] = sum;
+        sxr[warp] = xr;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (uint32_t w = 1; w < (blockDim.x >> 5); ++w) {
+            sum += ssum[w];
+            xr ^= sxr[w];
+        }
+        atomicAdd(acc, (unsigned long long)sum);
+        atomicXor(acc + 1, (unsigned long long)xr);
+    }
+}
+
 int grid_for(uint64_t work_items, uint32_t threads)
 {
     int dev = 0, sms = 148;
@@ -177,6 +246,28 @@ int pa_degrees(const pa_params *prm, const void *d_edges, int64_t *d_deg, void *
                                                             prm->n, (unsigned long long *)d_deg);
     }
     e = cudaGetLastError();
+    return e == cudaSuccess ? PA_OK : set_cuda_error(e);
+}
+
+int pa_digest(const void *d_ids, uint64_t count, uint32_t id_bits, uint64_t index_base,
+              uint64_t *d_acc, void *stream)
+{
+    if (!d_acc || (id_bits != 32 && id_bits != 64) || (count && !d_ids)) return PA_ERR_INVALID;
+    if (reinterpret_cast<uintptr_t>(d_acc) & 7u) return PA_ERR_INVALID;
+    if (!count) return PA_OK;
+    const uint32_t threads = 256;
+    const bool vec = (reinterpret_cast<uintptr_t>(d_ids) & 15u) == 0;
+    // Up to eight blocks of 256 threads per SM (grid_for): enough 16-byte loads
+    // in flight to stream at HBM speed; the grid never exceeds the work.
+    const int grid = grid_for(count / (vec ? 16u / (id_bits / 8u) : 1u) + 1, threads);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (id_bits == 64)
+        digest_kernel<int64_t><<<grid, threads, 0, s>>>((const int64_t *)d_ids, count, index_base,
+                                                        vec, (unsigned long long *)d_acc);
+    else
+        digest_kernel<int32_t><<<grid, threads, 0, s>>>((const int32_t *)d_ids, count, index_base,
+                                                        vec, (unsigned long long *)d_acc);
+    const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? PA_OK : set_cuda_error(e);
 }
 

@@ -177,6 +177,8 @@ _SIGS = {
                                        ctypes.c_void_p]),
     "pa_degrees": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_void_p,
                                   ctypes.c_void_p]),
+    "pa_digest": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32,
+                                 ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),
     "pa_csr_bytes": (ctypes.c_int, [_P(PaParams), _P(ctypes.c_uint64), _P(ctypes.c_uint64),
                                     _P(ctypes.c_uint64)]),
     "pa_build_csr": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_void_p,
@@ -436,6 +438,21 @@ def degrees(prm: PaParams, edges, stream=None):
                            ctypes.c_void_p(deg.data_ptr()),
                            ctypes.c_void_p(_stream_ptr(stream))), "pa_degrees")
     return deg
+
+
+def digest(ids, index_base: int = 0, stream=None) -> tuple[int, int]:
+    """pa_digest of a device tensor of int32/int64 ids taken as one flat array:
+    (sum, xor) of the position-keyed terms, as unsigned 64-bit integers."""
+    torch = _torch()
+    if ids.dtype not in (torch.int32, torch.int64) or not ids.is_contiguous():
+        raise ValueError("digest needs a contiguous int32 or int64 tensor")
+    acc = torch.zeros(2, dtype=torch.int64, device=ids.device)
+    check(lib().pa_digest(ctypes.c_void_p(ids.data_ptr()), ids.numel(),
+                          32 if ids.dtype == torch.int32 else 64, index_base,
+                          ctypes.c_void_p(acc.data_ptr()), ctypes.c_void_p(_stream_ptr(stream))),
+          "pa_digest")
+    a, b = acc.tolist()
+    return a & (2 ** 64 - 1), b & (2 ** 64 - 1)
 
 
 def build_csr(prm: PaParams, edges, stream=None):

@@ -203,6 +203,19 @@ int pa_canonicalize(const pa_params *prm, const void *d_edges, void *d_out, void
 /* Undirected degree of every node: d_deg is int64[n]. */
 int pa_degrees(const pa_params *prm, const void *d_edges, int64_t *d_deg, void *stream);
 
+/* Position-keyed digest of `count` ids of id_bits width at d_ids: d_acc[0]
+ * (device uint64) gains the sum and d_acc[1] the xor of
+ *   h = fmix64(fmix64(pos * 0x9E3779B97F4A7C15 + 0x632BE59BD9B4E019) ^ x),
+ * x the id sign-extended to 64 bits, pos = index_base + i, fmix64 MurmurHash3's
+ * 64-bit finalizer.  A fingerprint of a whole graph that never leaves the
+ * device: pass an edge list as 2 * pa_edge_count() ids (src of edge e at 2e,
+ * dst at 2e+1), a CSR as its rowptr (64-bit) and col.  The digest of a
+ * concatenation is the sum and xor of its parts' digests taken with their
+ * index bases, so a graph can be digested in pieces; clear d_acc to start one.
+ * Queued on `stream`.  No counterpart in the reference. */
+int pa_digest(const void *d_ids, uint64_t count, uint32_t id_bits, uint64_t index_base,
+              uint64_t *d_acc, void *stream);
+
 /* ---- CSR ------------------------------------------------------------------ */
 /* Undirected CSR of a generated edge list (PAIRS layout, slot or canonical
  * order): every edge appears in both rows, and every row is sorted ascending.

@@ -131,128 +131,28 @@ static inline uint64_t mulhi64(uint64_t a, uint64_t b)
     return (uint64_t)(((unsigned __int128)a * b) >> 64);
 }
 
+/* Generation loops for int64 and int32 slot storage (pa_oracle_gen.inc). */
+#define SLOT_T int64_t
+#define GEN_FN(name) name##_i64
+#include "pa_oracle_gen.inc"
+#undef SLOT_T
+#undef GEN_FN
+#define SLOT_T int32_t
+#define GEN_FN(name) name##_i32
+#include "pa_oracle_gen.inc"
+#undef SLOT_T
+#undef GEN_FN
+
 int orc_generate(uint64_t n, uint32_t d, double p, uint64_t seed, int seed_mode, int rng,
                  int64_t *G, uint64_t *retries_out)
 {
-    if (d == 0 || n < (uint64_t)d + 1 || G == NULL) return -1;
-    if (seed_mode != ORC_SEED_STAR_REF && seed_mode != ORC_SEED_CLIQUE) return -1;
-    if (rng != ORC_RNG_PHILOX && rng != ORC_RNG_MT_REF) return -1;
-
-    for (uint64_t v = 0; v <= d; ++v)
-        for (uint32_t k = 0; k < d; ++k) G[v * d + k] = seed_slot(v, k, d, seed_mode);
-
-    uint64_t retries = 0;
-    if (rng == ORC_RNG_PHILOX) {
-        const uint64_t pth = orc_p_threshold(p);
-        const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
-        for (uint64_t u = (uint64_t)d + 1; u < n; ++u) {
-            int64_t *row = G + u * d;
-            for (uint32_t i = 0; i < d; ++i) {
-                for (uint32_t r = 0;; ++r) {
-                    const uint32_t ctr[4] = {(uint32_t)u, (uint32_t)(u >> 32), i, r};
-                    uint32_t w[4];
-                    orc_philox4x32_10(ctr, key, w);
-                    uint64_t v = mulhi64(((uint64_t)w[1] << 32) | w[0], u);
-                    int64_t cand;
-                    if ((uint64_t)w[2] < pth) {
-                        cand = (int64_t)v;
-                    } else {
-                        uint32_t k = (uint32_t)(((uint64_t)w[3] * d) >> 32);
-                        cand = G[v * d + k];
-                    }
-                    int dup = 0;
-                    for (uint32_t j = 0; j < i; ++j)
-                        if (row[j] == cand) { dup = 1; break; }
-                    if (!dup) { row[i] = cand; break; }
-                    ++retries;
-                }
-            }
-        }
-    } else {
-        /* The reference's own draw sequence: one global MT19937-64 stream with
-         * its default seed, R = U % Z then coin = U53 * 2^-53, for every try. */
-        mt64 m;
-        mt64_seed(&m, seed);
-        for (uint64_t u = (uint64_t)d + 1; u < n; ++u) {
-            int64_t *row = G + u * d;
-            const uint64_t Z = (uint64_t)d * u;
-            for (uint32_t i = 0; i < d; ++i) {
-                for (;;) {
-                    uint64_t R = mt64_next(&m) % Z;
-                    double coin = (double)(mt64_next(&m) >> 11) * (1.0 / 9007199254740992.0);
-                    int64_t cand = coin < p ? (int64_t)(R / d) : G[R];
-                    int dup = 0;
-                    for (uint32_t j = 0; j < i; ++j)
-                        if (row[j] == cand) { dup = 1; break; }
-                    if (!dup) { row[i] = cand; break; }
-                    ++retries;
-                }
-            }
-        }
-    }
-    if (retries_out) *retries_out = retries;
-    return 0;
-}
-
-/*
- * Repeated-nodes Barabasi-Albert (the reference's -A sba,
- * src/PA/SPA/SerialBA.cpp:68-186): node u picks d distinct targets uniformly
- * from the endpoint list of all earlier edges -- the seed block (node i < d
- * repeated 2d times) followed, per node w = d, d+1, ..., by [target_0, w,
- * target_1, w, ...] -- so a draw is R uniform in [0, Z_u), Z_u = 2d^2 +
- * 2d(u - d), decoded as: R < 2d^2 -> node R / 2d; else r = R - 2d^2, w = d +
- * r / 2d, q = r % 2d -> q odd: w itself, q even: the target in slot q/2 of w.
- * Node d's targets are 0..d-1 (the reference's initial set), which is the
- * STAR_REF seed row.  PHILOX: R = mulhi64(w1:w0, Z_u) of
- * Philox(ctr = (u_lo, u_hi, i, r)); MT_REF: R = U % Z_u from the reference's
- * MT19937-64 stream, one draw per try, nodes in order.
- */
-static int64_t ba_endpoint(uint64_t R, uint32_t d, const int64_t *G)
-{
-    const uint64_t seed_block = 2ull * d * d;
-    if (R < seed_block) return (int64_t)(R / (2ull * d));
-    const uint64_t r = R - seed_block;
-    const uint64_t w = d + r / (2ull * d);
-    const uint64_t q = r % (2ull * d);
-    return (q & 1) ? (int64_t)w : G[w * d + q / 2];
+    return generate_i64(n, d, p, seed, seed_mode, rng, G, retries_out);
 }
 
 int orc_generate_ba(uint64_t n, uint32_t d, uint64_t seed, int rng, int64_t *G,
                     uint64_t *retries_out)
 {
-    if (d == 0 || n < (uint64_t)d + 1 || G == NULL) return -1;
-    if (rng != ORC_RNG_PHILOX && rng != ORC_RNG_MT_REF) return -1;
-    for (uint64_t v = 0; v <= d; ++v)
-        for (uint32_t k = 0; k < d; ++k) G[v * d + k] = seed_slot(v, k, d, ORC_SEED_STAR_REF);
-    uint64_t retries = 0;
-    const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
-    mt64 m;
-    mt64_seed(&m, seed);
-    for (uint64_t u = (uint64_t)d + 1; u < n; ++u) {
-        int64_t *row = G + u * d;
-        const uint64_t Z = 2ull * d * d + 2ull * d * (u - d);
-        for (uint32_t i = 0; i < d; ++i) {
-            for (uint32_t r = 0;; ++r) {
-                uint64_t R;
-                if (rng == ORC_RNG_PHILOX) {
-                    const uint32_t ctr[4] = {(uint32_t)u, (uint32_t)(u >> 32), i, r};
-                    uint32_t w[4];
-                    orc_philox4x32_10(ctr, key, w);
-                    R = mulhi64(((uint64_t)w[1] << 32) | w[0], Z);
-                } else {
-                    R = mt64_next(&m) % Z;
-                }
-                const int64_t cand = ba_endpoint(R, d, G);
-                int dup = 0;
-                for (uint32_t j = 0; j < i; ++j)
-                    if (row[j] == cand) { dup = 1; break; }
-                if (!dup) { row[i] = cand; break; }
-                ++retries;
-            }
-        }
-    }
-    if (retries_out) *retries_out = retries;
-    return 0;
+    return generate_ba_i64(n, d, seed, rng, G, retries_out);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -348,6 +248,128 @@ void orc_csr(uint64_t n, uint32_t d, int seed_mode, const int64_t *G, int64_t *r
     }
     free(cur);
     free(pairs);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Whole-graph digests                                                       */
+/* ------------------------------------------------------------------------ */
+/* MurmurHash3's 64-bit finalizer (Appleby, public domain): a bijective mix. */
+static inline uint64_t fmix64(uint64_t k)
+{
+    k ^= k >> 33;
+    k *= 0xFF51AFD7ED558CCDULL;
+    k ^= k >> 33;
+    k *= 0xC4CEB9FE1A85EC53ULL;
+    k ^= k >> 33;
+    return k;
+}
+
+/* Term of element x at position pos: the position is mixed in first, so the
+ * digest changes when two elements trade places. */
+static inline uint64_t digest_term(uint64_t pos, uint64_t x)
+{
+    return fmix64(fmix64(pos * 0x9E3779B97F4A7C15ULL + 0x632BE59BD9B4E019ULL) ^ x);
+}
+
+static inline void digest_add(uint64_t acc[2], uint64_t pos, int64_t x)
+{
+    const uint64_t h = digest_term(pos, (uint64_t)x);
+    acc[0] += h;
+    acc[1] ^= h;
+}
+
+void orc_digest_ids(const int64_t *x, uint64_t count, uint64_t index_base, uint64_t acc[2])
+{
+    for (uint64_t i = 0; i < count; ++i) digest_add(acc, index_base + i, x[i]);
+}
+
+/* Canonical seed edges of row v <= d, targets ascending, into tmp; returns how many. */
+static uint32_t seed_row_targets(uint64_t v, uint32_t d, const int32_t *G, int64_t *tmp)
+{
+    uint32_t c = 0;
+    for (uint32_t k = 0; k < d; ++k)
+        if ((int64_t)G[v * d + k] < (int64_t)v) tmp[c++] = G[v * d + k];
+    sort_small(tmp, c);
+    return c;
+}
+
+int orc_graph_digests(uint64_t n, uint32_t d, double p, uint64_t seed, int seed_mode, int model,
+                      int with_csr, uint64_t out[7])
+{
+    if (d == 0 || n < (uint64_t)d + 1 || n > (1ULL << 31) || out == NULL) return -1;
+    if (model != ORC_MODEL_COPY && model != ORC_MODEL_BA) return -1;
+    int32_t *G = (int32_t *)malloc(sizeof(int32_t) * n * d);
+    int64_t *tmp = (int64_t *)malloc(sizeof(int64_t) * d);
+    if (!G || !tmp) { free(G); free(tmp); return -2; }
+    uint64_t retries = 0;
+    const int rc = model == ORC_MODEL_BA
+                       ? generate_ba_i32(n, d, seed, ORC_RNG_PHILOX, G, &retries)
+                       : generate_i32(n, d, p, seed, seed_mode, ORC_RNG_PHILOX, G, &retries);
+    if (rc != 0) { free(G); free(tmp); return rc; }
+    for (int i = 0; i < 7; ++i) out[i] = 0;
+    out[6] = retries;
+
+    /* PAIRS slot order as one flat id array: src of edge e at 2e, dst at 2e+1. */
+    uint64_t e = 0;
+    for (uint64_t v = 0; v <= d; ++v)
+        for (uint32_t k = 0; k < d; ++k) {
+            const int64_t w = G[v * d + k];
+            if (w < (int64_t)v) {
+                digest_add(out, 2 * e, (int64_t)v);
+                digest_add(out, 2 * e + 1, w);
+                ++e;
+            }
+        }
+    for (uint64_t u = (uint64_t)d + 1; u < n; ++u)
+        for (uint32_t i = 0; i < d; ++i, ++e) {
+            digest_add(out, 2 * e, (int64_t)u);
+            digest_add(out, 2 * e + 1, G[u * d + i]);
+        }
+
+    if (with_csr) {
+        /* rp[x] = row start (degrees, then an exclusive scan). */
+        uint64_t *rp = (uint64_t *)calloc(n + 1, sizeof(uint64_t));
+        if (!rp) { free(G); free(tmp); return -2; }
+        for (uint64_t v = 0; v <= d; ++v)
+            for (uint32_t k = 0; k < d; ++k) {
+                const int64_t w = G[v * d + k];
+                if (w < (int64_t)v) { rp[v + 1]++; rp[w + 1]++; }
+            }
+        for (uint64_t u = (uint64_t)d + 1; u < n; ++u) {
+            rp[u + 1] += d;
+            for (uint32_t i = 0; i < d; ++i) rp[(uint64_t)G[u * d + i] + 1]++;
+        }
+        for (uint64_t x = 0; x < n; ++x) rp[x + 1] += rp[x];
+        for (uint64_t x = 0; x <= n; ++x) digest_add(out + 2, x, (int64_t)rp[x]);
+        /* Out parts: row x's own targets (< x) ascending at the row's start; the
+         * row start then becomes the cursor of its in part. */
+        for (uint64_t x = 0; x < n; ++x) {
+            uint32_t c;
+            if (x <= d) {
+                c = seed_row_targets(x, d, G, tmp);
+            } else {
+                for (uint32_t i = 0; i < d; ++i) tmp[i] = G[x * d + i];
+                sort_small(tmp, d);
+                c = d;
+            }
+            for (uint32_t j = 0; j < c; ++j) digest_add(out + 4, rp[x] + j, tmp[j]);
+            rp[x] += c;
+        }
+        /* In parts: every u > v in increasing u, appended to row v. */
+        for (uint64_t u = 1; u < n; ++u) {
+            if (u <= d) {
+                const uint32_t c = seed_row_targets(u, d, G, tmp);
+                for (uint32_t j = 0; j < c; ++j) digest_add(out + 4, rp[tmp[j]]++, (int64_t)u);
+            } else {
+                for (uint32_t i = 0; i < d; ++i)
+                    digest_add(out + 4, rp[(uint64_t)G[u * d + i]]++, (int64_t)u);
+            }
+        }
+        free(rp);
+    }
+    free(tmp);
+    free(G);
+    return 0;
 }
 
 uint64_t orc_fnv1a64(const void *data, uint64_t bytes)

@@ -94,6 +94,32 @@ void orc_degrees(uint64_t n, uint32_t d, int seed_mode, const int64_t *G, int64_
 void orc_csr(uint64_t n, uint32_t d, int seed_mode, const int64_t *G, int64_t *rowptr,
              int64_t *col);
 
+/*
+ * Position-keyed digest of an id array: acc[0] += h, acc[1] ^= h over
+ * h = fmix64(fmix64(pos * 0x9E3779B97F4A7C15 + 0x632BE59BD9B4E019) ^ x) for every
+ * element x at pos = index_base + i (fmix64: MurmurHash3's finalizer).  The
+ * digest of a concatenation is the sum / xor of the digests of its parts with
+ * their index bases, so it can be taken chunk by chunk; swapping two elements
+ * changes it.  acc is accumulated into, not cleared.
+ */
+void orc_digest_ids(const int64_t *x, uint64_t count, uint64_t index_base, uint64_t acc[2]);
+
+enum { ORC_MODEL_COPY = 0, ORC_MODEL_BA = 1 };
+
+/*
+ * Whole-graph digests of a Philox-mode graph of n <= 2^31 nodes, generated with
+ * int32 slot storage (n*d*4 bytes of host memory, plus 8*(n+1) with CSR):
+ *   out[0..1]  the PAIRS slot-order edge list as one flat id array
+ *              (src of edge e at 2e, dst at 2e+1);
+ *   out[2..3]  the undirected CSR's rowptr[0..n];
+ *   out[4..5]  the CSR's col[0..2E) (out[2..5] stay zero unless with_csr);
+ *   out[6]     the number of rejected draws.
+ * model: ORC_MODEL_COPY (seed_mode as given) or ORC_MODEL_BA (STAR_REF seed).
+ * Returns 0, -1 on invalid arguments, -2 when host memory runs out.
+ */
+int orc_graph_digests(uint64_t n, uint32_t d, double p, uint64_t seed, int seed_mode, int model,
+                      int with_csr, uint64_t out[7]);
+
 /* 64-bit FNV-1a over a byte buffer (fixture digests). */
 uint64_t orc_fnv1a64(const void *data, uint64_t bytes);
 

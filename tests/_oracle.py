@@ -48,6 +48,9 @@ def lib() -> ctypes.CDLL:
         for f in ("orc_pairs_slot_order", "orc_pairs_canonical", "orc_degrees"):
             getattr(L, f).argtypes = [_u64, _u32, _i, _vp, _vp]
         L.orc_csr.argtypes = [_u64, _u32, _i, _vp, _vp, _vp]
+        L.orc_digest_ids.argtypes = [_vp, _u64, _u64, _vp]
+        L.orc_graph_digests.argtypes = [_u64, _u32, ctypes.c_double, _u64, _i, _i, _i, _vp]
+        L.orc_graph_digests.restype = _i
         L.orc_fnv1a64.argtypes = [_vp, _u64]
         L.orc_fnv1a64.restype = _u64
         _lib = L
@@ -140,6 +143,29 @@ def csr(G: np.ndarray, seed_mode: int):
 def fnv1a64(a: np.ndarray) -> int:
     a = np.ascontiguousarray(a)
     return int(lib().orc_fnv1a64(a.ctypes.data, a.nbytes))
+
+
+MODEL_COPY = 0
+MODEL_BA = 1
+
+
+def digest_ids(a: np.ndarray, index_base: int = 0, acc=(0, 0)) -> tuple[int, int]:
+    """Position-keyed (sum, xor) digest of a flat id array (orc_digest_ids)."""
+    a = np.ascontiguousarray(np.asarray(a).reshape(-1), dtype=np.int64)
+    out = (ctypes.c_uint64 * 2)(*acc)
+    lib().orc_digest_ids(a.ctypes.data, a.size, index_base, out)
+    return int(out[0]), int(out[1])
+
+
+def graph_digests(n: int, d: int, p: float, seed: int, seed_mode: int = SEED_CLIQUE,
+                  model: int = MODEL_COPY, with_csr: bool = False) -> dict:
+    """Whole-graph digests without materialising the edge list (orc_graph_digests)."""
+    out = (ctypes.c_uint64 * 7)()
+    rc = lib().orc_graph_digests(n, d, p, seed, seed_mode, model, int(with_csr), out)
+    if rc != 0:
+        raise ValueError(f"oracle digest failed ({rc}) for n={n} d={d} p={p}")
+    return {"pairs": (int(out[0]), int(out[1])), "rowptr": (int(out[2]), int(out[3])),
+            "col": (int(out[4]), int(out[5])), "retries": int(out[6])}
 
 
 def dd_csv_from_degrees(deg: np.ndarray) -> str:

@@ -20,9 +20,16 @@ Two kinds of fixture:
 2. Oracle digests.  FNV-1a 64 of the oracle's Philox-mode edge lists (slot
    order and canonical, int64 little-endian) for a fixed list of shapes, plus one
    tiny full edge list.  They pin the oracle itself across edits.
+3. Whole-graph digests of the benchmark configurations at full size
+   (`python tests/golden/make_golden.py fullsize`, about half an hour on one
+   core per configuration, up to 26 GB of host memory each): the oracle's
+   position-keyed digests (orc_graph_digests) of the PAIRS edge list and, where
+   listed, of the CSR's rowptr and col.  The GPU tests and bench.py compare the
+   device's digest of its own output against these.
 
 Needs the reference tree only for part 1 (scm_ref and sba_ref must already be
-built).
+built).  With arguments, only the named parts run (scm, sba, write, digest,
+ba_digest, fullsize).
 """
 from __future__ import annotations
 
@@ -160,10 +167,59 @@ def digest_fixtures():
         f.writelines(f"{u} {v}\n" for u, v in can.tolist())
 
 
+# Full-size configurations: (name, n, d, p, seed, seed_mode, model, with_csr).
+FULLSIZE_CASES = [
+    ("c3_p0.5", 2 ** 30, 4, 0.5, 1234, orc.SEED_CLIQUE, orc.MODEL_COPY, True),
+    ("c2", 10 ** 8, 16, 0.5, 7, orc.SEED_CLIQUE, orc.MODEL_COPY, True),
+    ("c3_p0", 2 ** 30, 4, 0.0, 1234, orc.SEED_CLIQUE, orc.MODEL_COPY, False),
+    ("sba_n2^30", 2 ** 30, 4, 0.0, 1234, orc.SEED_STAR_REF, orc.MODEL_BA, False),
+]
+
+
+def _fullsize_one(case):
+    import time
+    name, n, d, p, seed, mode, model, with_csr = case
+    t0 = time.time()
+    dg = orc.graph_digests(n, d, p, seed, mode, model, with_csr)
+    rec = {"name": name, "n": n, "d": d, "p": p, "seed": seed, "seed_mode": mode,
+           "model": model, "edges": orc.edge_count(n, d, mode if model == orc.MODEL_COPY
+                                                     else orc.SEED_STAR_REF),
+           "retries": dg["retries"], "pairs": [f"{x:016x}" for x in dg["pairs"]],
+           "oracle_seconds": round(time.time() - t0, 1)}
+    if with_csr:
+        rec["rowptr"] = [f"{x:016x}" for x in dg["rowptr"]]
+        rec["col"] = [f"{x:016x}" for x in dg["col"]]
+    return rec
+
+
+def fullsize_fixtures(workers: int = 2):
+    """Runs the cases in `workers` spawned processes (host memory bounds it)."""
+    import multiprocessing as mp
+    path = os.path.join(HERE, "fullsize_digests.json")
+    done = {}
+    if os.path.exists(path):
+        with open(path) as f:
+            done = {c["name"]: c for c in json.load(f)["cases"]}
+    todo = [c for c in FULLSIZE_CASES if c[0] not in done]
+    with mp.get_context("spawn").Pool(workers) as pool:
+        for rec in pool.imap_unordered(_fullsize_one, todo):
+            done[rec["name"]] = rec
+            order = [c[0] for c in FULLSIZE_CASES]
+            with open(path, "w") as f:
+                json.dump({"digest": "orc_digest_ids: sum and xor (hex) of "
+                                     "fmix64(fmix64(pos*0x9E3779B97F4A7C15 + 0x632BE59BD9B4E019) ^ id) "
+                                     "over a flat id array (PAIRS: src at 2e, dst at 2e+1; "
+                                     "CSR rowptr[0..n], col[0..2E)); Philox mode",
+                           "cases": [done[k] for k in order if k in done]}, f, indent=1)
+            print("fullsize", rec["name"], rec["oracle_seconds"], "s", flush=True)
+
+
+PARTS = {"scm": scm_fixtures, "sba": sba_fixtures, "write": write_fixture,
+         "digest": digest_fixtures, "ba_digest": ba_digest_fixtures,
+         "fullsize": fullsize_fixtures}
+
 if __name__ == "__main__":
-    scm_fixtures()
-    sba_fixtures()
-    write_fixture()
-    digest_fixtures()
-    ba_digest_fixtures()
+    names = sys.argv[1:] or ["scm", "sba", "write", "digest", "ba_digest"]
+    for name in names:
+        PARTS[name]()
     print("fixtures written to", HERE)

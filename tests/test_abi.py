@@ -171,3 +171,14 @@ def test_binding_fails_loudly_without_the_library(pa, monkeypatch, tmp_path):
     monkeypatch.setattr(pa, "_lib", None)
     with pytest.raises(FileNotFoundError):
         pa.lib()
+
+
+def test_digest_rejects_bad_arguments_without_touching_the_device(pa):
+    L = pa.lib()
+    acc = ctypes.c_void_p(4096)          # never dereferenced: every call below is refused
+    assert L.pa_digest(ctypes.c_void_p(4096), 10, 64, 0, None, None) == pa.PA_ERR_INVALID
+    assert L.pa_digest(ctypes.c_void_p(4096), 10, 16, 0, acc, None) == pa.PA_ERR_INVALID
+    assert L.pa_digest(None, 10, 64, 0, acc, None) == pa.PA_ERR_INVALID
+    assert L.pa_digest(ctypes.c_void_p(4096), 10, 64, 0, ctypes.c_void_p(4100), None) == \
+        pa.PA_ERR_INVALID
+    assert L.pa_digest(None, 0, 32, 0, acc, None) == pa.PA_OK     # nothing to do

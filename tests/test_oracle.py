@@ -327,3 +327,79 @@ def test_text_format_is_the_reference_writers():
     text = "".join(f"{u} {v}\n" for u, v in orc.pairs_slot_order(G, orc.SEED_STAR_REF).tolist())
     with open(os.path.join(GOLD, f"ref_write_n{n}_m{m}_p{p}.txt")) as f:
         assert text == f.read()
+
+
+# ---------------------------------------------------------------------------
+# Whole-graph digests (orc_digest_ids, orc_graph_digests)
+
+_M64 = (1 << 64) - 1
+
+
+def _fmix64_py(k):
+    k ^= k >> 33
+    k = (k * 0xFF51AFD7ED558CCD) & _M64
+    k ^= k >> 33
+    k = (k * 0xC4CEB9FE1A85EC53) & _M64
+    return k ^ (k >> 33)
+
+
+def _digest_py(ids, base=0):
+    """The digest's definition, restated in plain Python integers."""
+    s = x = 0
+    for i, v in enumerate(ids):
+        h = _fmix64_py(_fmix64_py(((base + i) * 0x9E3779B97F4A7C15 + 0x632BE59BD9B4E019) & _M64)
+                       ^ (int(v) & _M64))
+        s = (s + h) & _M64
+        x ^= h
+    return s, x
+
+
+def test_digest_definition():
+    ids = np.array([0, 1, 2, 7, -1, 2 ** 40 + 3, 5, 5, 123456789], dtype=np.int64)
+    assert orc.digest_ids(ids) == _digest_py(ids.tolist())
+    assert orc.digest_ids(ids, 1000) == _digest_py(ids.tolist(), 1000)
+    # position-keyed: swapping two elements changes it
+    sw = ids.copy()
+    sw[[1, 2]] = sw[[2, 1]]
+    assert orc.digest_ids(sw) != orc.digest_ids(ids)
+    # pieces with their index bases add up to the whole
+    a = orc.digest_ids(ids[:4])
+    b = orc.digest_ids(ids[4:], 4)
+    assert ((a[0] + b[0]) & _M64, a[1] ^ b[1]) == orc.digest_ids(ids)
+
+
+@pytest.mark.parametrize("n,d,p,seed,mode,model", [
+    (3000, 4, 0.5, 42, orc.SEED_CLIQUE, orc.MODEL_COPY),
+    (3000, 4, 0.5, 42, orc.SEED_STAR_REF, orc.MODEL_COPY),
+    (2000, 7, 0.2, 5, orc.SEED_CLIQUE, orc.MODEL_COPY),
+    (2000, 1, 0.5, 3, orc.SEED_CLIQUE, orc.MODEL_COPY),
+    (1500, 4, 0.0, 1234, orc.SEED_CLIQUE, orc.MODEL_COPY),
+    (500, 32, 0.9, 2, orc.SEED_CLIQUE, orc.MODEL_COPY),
+    (3000, 4, 0.0, 9, orc.SEED_STAR_REF, orc.MODEL_BA),
+])
+def test_graph_digests_equal_the_materialised_outputs(n, d, p, seed, mode, model):
+    """The streaming whole-graph digests (int32 slots, no edge list in memory)
+    equal the digests of the int64 oracle's edge list and CSR."""
+    dg = orc.graph_digests(n, d, p, seed, mode, model, with_csr=True)
+    if model == orc.MODEL_BA:
+        G, r = orc.generate_ba(n, d, seed, with_retries=True)
+    else:
+        G, r = orc.generate(n, d, p, seed, mode, with_retries=True)
+    pairs = orc.pairs_slot_order(G, mode)
+    rowptr, col = orc.csr(G, mode)
+    assert dg["pairs"] == orc.digest_ids(pairs)
+    assert dg["rowptr"] == orc.digest_ids(rowptr)
+    assert dg["col"] == orc.digest_ids(col)
+    assert dg["retries"] == r
+
+
+def test_fullsize_digest_fixture_is_complete():
+    """The committed whole-graph digests of the benchmark configurations."""
+    with open(os.path.join(GOLD, "fullsize_digests.json")) as f:
+        cases = {c["name"]: c for c in json.load(f)["cases"]}
+    for name in ("c3_p0.5", "c3_p0", "c2"):
+        c = cases[name]
+        assert c["edges"] == orc.edge_count(c["n"], c["d"], c["seed_mode"])
+        assert len(c["pairs"]) == 2 and all(len(h) == 16 for h in c["pairs"])
+    for name in ("c3_p0.5", "c2"):
+        assert "rowptr" in cases[name] and "col" in cases[name]

@@ -24,7 +24,18 @@ Besides the device-timed value the line carries:
   roofline     algorithmic bytes of the generator kernel per launch over its
                CUDA-event duration, against the measured HBM copy bandwidth;
   cpu_baseline the sequential CPU oracle on a bounded sample (1 core);
-  clocks       SM clocks and throttle reasons sampled during the timed region.
+  clocks       SM clocks and throttle reasons sampled during the timed region;
+  parity       after the timed region, the device digest (pa_digest) of the
+               last step's whole edge list against the oracle's digest of the
+               same configuration (tests/golden/fullsize_digests.json);
+  step_dram_frac  the whole step (kernel traffic from the committed ncu
+               capture plus the all-ones fill) in DRAM bytes over the step
+               time, against the same peak;
+  batched, served  (default workload, one GPU) the batched and served figures
+               of the metric: 4,096 mixed instances in one persistent launch per
+               wave against one launch per graph, and Poisson request streams
+               through the request server at 2,000 req/s (a 2 s window) and at
+               a sustainable 100 req/s (5 s), with p50/p99 latency.
 
 --impl reference times the reference's own sequential generator
 (oracle/_ref/scm_ref, src/PA/SPA/SerialCopyModel3.cpp compiled from the
@@ -49,22 +60,23 @@ sys.path.insert(0, os.path.join(ROOT, "cuppa-public_b200"))
 CLIQUE, STAR_REF = 1, 0
 COPY, BA = 0, 1
 WORKLOADS = {
-    "c3": dict(n=2 ** 30, d=4, p=0.5, seed=1234, id_bits=64, seed_mode=CLIQUE,
+    "c3": dict(n=2 ** 30, d=4, p=0.5, seed=1234, id_bits=64, seed_mode=CLIQUE, fixture="c3_p0.5",
                name="copy-model PA, n=2^30, d=4, p=0.5, int64 ids, clique seed, Philox seed 1234"),
-    "c3p0": dict(n=2 ** 30, d=4, p=0.0, seed=1234, id_bits=64, seed_mode=CLIQUE,
+    "c3p0": dict(n=2 ** 30, d=4, p=0.0, seed=1234, id_bits=64, seed_mode=CLIQUE, fixture="c3_p0",
                  name="copy-model PA, n=2^30, d=4, p=0.0, int64 ids, clique seed, Philox seed 1234"),
-    "c2": dict(n=10 ** 8, d=16, p=0.5, seed=7, id_bits=64, seed_mode=CLIQUE,
+    "c2": dict(n=10 ** 8, d=16, p=0.5, seed=7, id_bits=64, seed_mode=CLIQUE, fixture="c2",
                name="copy-model PA, n=10^8, d=16, p=0.5, int64 ids, clique seed, Philox seed 7"),
-    "c3s": dict(n=2 ** 25, d=4, p=0.5, seed=1234, id_bits=64, seed_mode=CLIQUE,
+    "c3s": dict(n=2 ** 25, d=4, p=0.5, seed=1234, id_bits=64, seed_mode=CLIQUE, fixture="c3s",
                 name="copy-model PA, n=2^25, d=4, p=0.5, int64 ids, clique seed, Philox seed 1234 "
                      "(profiling size)"),
-    "c3m": dict(n=2 ** 26, d=4, p=0.5, seed=1234, id_bits=64, seed_mode=CLIQUE,
+    "c3m": dict(n=2 ** 26, d=4, p=0.5, seed=1234, id_bits=64, seed_mode=CLIQUE, fixture="c3m",
                 name="copy-model PA, n=2^26, d=4, p=0.5, int64 ids, clique seed, Philox seed 1234 "
                      "(traffic capture size)"),
-    "c1": dict(n=10 ** 5, d=4, p=0.5, seed=42, id_bits=32, seed_mode=CLIQUE,
+    "c1": dict(n=10 ** 5, d=4, p=0.5, seed=42, id_bits=32, seed_mode=CLIQUE, fixture="c1",
                name="copy-model PA, n=10^5, d=4, p=0.5, int32 ids, clique seed, Philox seed 42"),
     # the repeated-nodes Barabasi-Albert model of -A sba at the same size
     "sba": dict(n=2 ** 30, d=4, p=0.0, seed=1234, id_bits=64, seed_mode=STAR_REF, model=BA,
+                fixture="sba_n2^30",
                 name="repeated-nodes BA (-A sba), n=2^30, d=4, int64 ids, star seed, "
                      "Philox seed 1234",
                 metric="edges/s on 1 B200 (BA PA generation)"),
@@ -101,6 +113,22 @@ def load_traffic(workload: str):
         return t.get(workload, {}).get("dram_bytes_per_launch")
     except Exception:
         return None
+
+
+def load_fixture_digests(name):
+    """The oracle's whole-graph digests of a configuration (committed fixture
+    tests/golden/fullsize_digests.json, written by tests/golden/make_golden.py);
+    None when the configuration has none."""
+    path = os.path.join(ROOT, "tests", "golden", "fullsize_digests.json")
+    try:
+        with open(path) as f:
+            cases = {c["name"]: c for c in json.load(f)["cases"]}
+    except Exception:
+        return None
+    c = cases.get(name)
+    if c is None:
+        return None
+    return {k: tuple(int(x, 16) for x in c[k]) for k in ("pairs", "rowptr", "col") if k in c}
 
 
 class ClockSampler:
@@ -393,6 +421,21 @@ def run_gpu(args, w):
                      "ms_per_step": 1e3 * g_s / args.steps,
                      "plain_ms_per_step": 1e3 * e2e_s / args.steps}
 
+    # ---- parity of the last timed step's output (after all timing): the
+    # device digest of the whole edge list against the oracle's
+    want = load_fixture_digests(w.get("fixture"))
+    parity = None
+    if want is not None:
+        got = pa.digest(edges[:E].reshape(-1), stream=stream)
+        ok = got == want["pairs"]
+        if world > 1:
+            flag = torch.tensor([0.0 if ok else 1.0], device="cuda")
+            dist.all_reduce(flag)
+            ok = flag.item() == 0.0
+        parity = ok
+    elif world > 1:
+        dist.all_reduce(torch.zeros(1, device="cuda"))     # same collective steps on every rank
+
     if rank == 0:
         peak, peak_kind = load_peaks()
         bpe = algorithmic_bytes_per_edge(w)
@@ -435,21 +478,41 @@ def run_gpu(args, w):
             "gpu_launches": launches * args.steps,
             "clocks": clk.summary(),
             "device_stats": st.as_dict(),
+            "parity": parity,
+            "parity_check": ("device pa_digest of the whole edge list of the last timed step "
+                             "(2E ids, position-keyed) equal to the oracle's digest of the same "
+                             f"configuration (tests/golden/fullsize_digests.json, '{w.get('fixture')}')"
+                             if want is not None else "no whole-graph fixture for this workload"),
         }
+        # the whole step in actual DRAM bytes: the kernel's ncu traffic plus the
+        # all-ones fill of the start region (written once) over the step time
+        fill_bytes = (u_split - (w["d"] + 1)) * w["d"] * 2 * (w["id_bits"] // 8)
+        if traffic:
+            step_bytes = traffic + fill_bytes
+            line["step_dram_frac"] = step_bytes / (ms / args.steps / 1e3) / 1e9 / peak
+            line["step_dram"] = {"bytes": step_bytes, "kernel_traffic": traffic,
+                                 "fill_bytes": fill_bytes,
+                                 "gbs": step_bytes / (ms / args.steps / 1e3) / 1e9,
+                                 "peak": peak}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_oracle(w, CPU_SAMPLE_NODES)
+    del edges, scratch
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    if rank == 0 and world == 1 and args.workload == "c3" and not args.no_extras:
+        # the batched and served figures of the metric, measured in the same run
+        line["batched"] = measure_batched(args, 1, 0)[0]
+        line["served"] = {
+            "overload": measure_served(args, args.rate, args.serve_window, "csr", 1, 0)[0],
+            "sustainable": measure_served(args, args.sustain_rate, args.sustain_seconds, "csr",
+                                          1, 0)[0],
+        }
+    if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
-    return 0
-
-
-def _edge_hash(torch, e):
-    """Order-sensitive 64-bit digest of an edge tensor, computed on the device."""
-    x = e.reshape(-1).to(torch.int64)
-    idx = torch.arange(x.numel(), device=x.device, dtype=torch.int64)
-    return int(((x * 0x9E3779B97F4A7C15 + idx * 0xC2B2AE3D27D4EB4F) ^ (x >> 7)).sum().item())
+    return 0 if parity in (None, True) else 1
 
 
 STREAM_W = dict(n=2 ** 30, d=4, p=0.5, seed=1234, id_bits=64, seed_mode=CLIQUE,
@@ -584,21 +647,17 @@ def rank_share(pa, prms, world: int, rank: int) -> list:
     return [i for i, p in enumerate(part) if p == rank]
 
 
-def run_batched(args):
+def measure_batched(args, world: int, rank: int):
     """4,096 mixed instances: one persistent launch per wave vs one launch per
     graph, identical outputs checked by digest; graphs/s of both.  With N ranks
     the instances are split by pa_batch_partition and each rank runs its part
-    (the total is fixed: strong scaling; no collective beyond the timing)."""
+    (the total is fixed: strong scaling; no collective beyond the timing).
+    Returns (figures, identical) on every rank."""
     import torch
     import torch.distributed as dist
     import cuppa_b200 as pa
     from cuppa_b200.workloads import batched_instances, edges_of
 
-    world, rank, local = dist_setup()
-    torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
     inst = batched_instances(args.instances)
 
     def prm(i):
@@ -624,7 +683,7 @@ def run_batched(args):
     t_batch = t_plain = 0.0
     digests_b, digests_p = {}, {}
     total_edges = 0
-    with ClockSampler(0) as clk:
+    with ClockSampler(torch.cuda.current_device()) as clk:
         for wave in waves:
             prms = [prm(i) for i in wave]
             total_edges += sum(pa.edge_count(q) for q in prms)
@@ -640,7 +699,7 @@ def run_batched(args):
             t_batch += time.perf_counter() - t0
             pa.check(st.status, "batched generation")
             for k, i in enumerate(wave):
-                digests_b[i] = _edge_hash(torch, batch.graph(k))
+                digests_b[i] = pa.digest(batch.graph(k).reshape(-1), stream=stream)
             # plain: one pa_generate per graph, back to back on one stream
             scratch = torch.empty(max(pa.sizes(q)[1] for q in prms), dtype=torch.uint8,
                                   device="cuda")
@@ -652,7 +711,7 @@ def run_batched(args):
             t_plain += time.perf_counter() - t0
             pa.check(st.status, "plain generation")
             for k, i in enumerate(wave):
-                digests_p[i] = _edge_hash(torch, batch.graph(k))
+                digests_p[i] = pa.digest(batch.graph(k).reshape(-1), stream=stream)
             del batch, scratch
             torch.cuda.empty_cache()
     same = all(digests_b[i] == digests_p[i] for i in digests_b)
@@ -663,32 +722,56 @@ def run_batched(args):
         flags = torch.tensor([0.0 if same else 1.0, float(total_edges)], device="cuda")
         dist.all_reduce(flags)
         same, total_edges = flags[0].item() == 0.0, int(flags[1].item())
+    fig = {
+        "workload": f"{n_graphs} instances: n=round(10^U(3,7)), d=U{{1..32}}, p=U(0.1,0.9), "
+                    "seed=1000+i, int32, clique seed",
+        "graphs_per_s": n_graphs / t_batch, "ms": t_batch * 1e3,
+        "plain_graphs_per_s": n_graphs / t_plain, "plain_ms": t_plain * 1e3,
+        "speedup_vs_plain": t_plain / t_batch, "identical_outputs": same,
+        "edges": total_edges, "edges_per_s": total_edges / t_batch,
+        "waves_rank0": len(waves), "wave_budget_gb": args.budget_gb,
+        "timing": "host clock around each wave's launches and its completion wait",
+        "clocks": clk.summary(),
+    }
+    return fig, same
+
+
+def run_batched(args):
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    fig, same = measure_batched(args, world, rank)
+    if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
         return 0 if same else 1
     line = {
         "metric": "graphs/s, batched mixed instances (one persistent launch per wave)",
-        "value": n_graphs / t_batch, "unit": "graphs/s", "n_gpus": world, "steps": 1,
-        "warmup": args.warmup, "ms_per_step": t_batch * 1e3, "higher_is_better": True,
+        "value": fig["graphs_per_s"], "unit": "graphs/s", "n_gpus": world, "steps": 1,
+        "warmup": args.warmup, "ms_per_step": fig["ms"], "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (generator parameters only)",
-        "config": {"workload": f"{n_graphs} instances: n=round(10^U(3,7)), d=U{{1..32}}, "
-                               "p=U(0.1,0.9), seed=1000+i, int32, clique seed",
-                   "edges": total_edges, "waves_rank0": len(waves),
-                   "wave_budget_gb": args.budget_gb,
+        "config": {"workload": fig["workload"], "edges": fig["edges"],
+                   "waves_rank0": fig["waves_rank0"], "wave_budget_gb": args.budget_gb,
                    "parallelism": f"instances split over {world} ranks (pa_batch_partition)"
                    if world > 1 else "single"},
-        "plain_graphs_per_s": n_graphs / t_plain, "plain_ms": t_plain * 1e3,
-        "speedup_vs_plain": t_plain / t_batch, "identical_outputs": same,
-        "edges_per_s_batched": total_edges / t_batch,
-        "clocks": clk.summary(),
+        "plain_graphs_per_s": fig["plain_graphs_per_s"], "plain_ms": fig["plain_ms"],
+        "speedup_vs_plain": fig["speedup_vs_plain"], "identical_outputs": same,
+        "edges_per_s_batched": fig["edges_per_s"],
+        "clocks": fig["clocks"],
     }
     print(json.dumps(line), flush=True)
     return 0 if same else 1
 
 
-def run_served(args):
+def measure_served(args, rate: float, seconds: float, outputs_name: str, world: int,
+                   rank: int):
     """Poisson request stream through the request server (pa_server_*): requests
     are submitted at their arrival times from one thread, results are waited
     for and released in submission order from another; latency is the server's
@@ -696,19 +779,14 @@ def run_served(args):
     With N ranks, rank r serves the requests whose index is r mod N (a round-robin
     router: one server per GPU, no collective on the data path); the job's value
     is all ranks' edges over the slowest rank's span, and p50/p99 are over all
-    requests."""
+    requests.  Returns (figures, all_ok) on every rank."""
     import queue
     import torch
     import torch.distributed as dist
     import cuppa_b200 as pa
-    from cuppa_b200.workloads import serve_requests
+    from cuppa_b200.workloads import edges_of, serve_requests
 
-    world, rank, local = dist_setup()
-    torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
-    all_reqs = serve_requests(args.serve_seconds, args.rate)
+    all_reqs = serve_requests(seconds, rate)
     reqs = [r for i, r in enumerate(all_reqs) if i % world == rank]
     free_b, _ = torch.cuda.mem_get_info()
     budget = min(int(args.serve_budget_gb * 1e9), int(free_b * 0.9))
@@ -717,8 +795,9 @@ def run_served(args):
     tickets = queue.Queue()
     lat, edges_done, statuses = [], 0, []
     outputs = {"pairs": pa.PA_OUT_PAIRS, "csr": pa.PA_OUT_CSR,
-               "both": pa.PA_OUT_PAIRS | pa.PA_OUT_CSR}[args.serve_outputs]
-    with pa.Server(budget_bytes=budget, outputs=outputs) as srv, ClockSampler(local) as clk:
+               "both": pa.PA_OUT_PAIRS | pa.PA_OUT_CSR}[outputs_name]
+    with pa.Server(budget_bytes=budget, outputs=outputs) as srv, \
+            ClockSampler(torch.cuda.current_device()) as clk:
         # warm-up: a few requests, waited for and released
         for q in prms[: args.warmup]:
             t = srv.submit(q)
@@ -765,34 +844,62 @@ def run_served(args):
         edges_done = sum(g[1] for g in gathered)
         ok = all(g[2] for g in gathered)
         n_req = sum(g[3] for g in gathered)
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank != 0:
-        return 0 if ok else 1
     lat_sorted = sorted(lat)
 
     def pct(x):
         return lat_sorted[min(len(lat_sorted) - 1, int(round(x / 100 * (len(lat_sorted) - 1))))]
 
-    line = {
-        "metric": "served edges/s with p50/p99 latency (continuous batching)",
-        "value": edges_done / span_s, "unit": "edges/s", "n_gpus": world, "steps": 1,
-        "warmup": args.warmup, "ms_per_step": span_s * 1e3, "higher_is_better": True,
-        "scaling": "strong", "vs_baseline": None, "dtype": "int32",
-        "data": "synthetic (generator parameters only)",
-        "config": {"workload": f"Poisson {args.rate:g} req/s for {args.serve_seconds:g} s: "
-                               "n=round(10^U(4,8)), d=U{2..16}, p=U(0.2,0.8), int32, clique seed",
-                   "requests": n_req, "budget_gb_per_gpu": budget / 1e9,
-                   "parallelism": f"requests round-robin over {world} servers (one per rank)"
-                   if world > 1 else "single",
-                   "output": {"pairs": "edge list (PAIRS)", "csr": "undirected CSR",
-                              "both": "edge list and undirected CSR"}[args.serve_outputs]
-                             + " kept on the device until released"},
-        "p50_ms": pct(50), "p99_ms": pct(99), "max_ms": lat_sorted[-1],
-        "requests_per_s": n_req / span_s, "all_ok": ok, "server_stats_rank0": st,
+    offered_edges = sum(edges_of(r["n"], r["d"]) for r in all_reqs)
+    fig = {
+        "workload": f"Poisson {rate:g} req/s for {seconds:g} s: n=round(10^U(4,8)), d=U{{2..16}}, "
+                    "p=U(0.2,0.8), int32, clique seed",
+        "output": {"pairs": "edge list (PAIRS)", "csr": "undirected CSR",
+                   "both": "edge list and undirected CSR"}[outputs_name]
+                  + " kept on the device until released",
+        "requests": n_req, "window_s": seconds, "budget_gb_per_gpu": budget / 1e9,
+        "offered_requests_per_s": rate, "offered_edges_per_s": offered_edges / seconds,
+        "served_requests_per_s": n_req / span_s, "edges_per_s": edges_done / span_s,
+        "span_s": span_s, "p50_ms": pct(50), "p99_ms": pct(99), "max_ms": lat_sorted[-1],
+        "all_ok": ok, "server_stats_rank0": st,
         "statuses_rank0": {str(c): statuses.count(c) for c in sorted(set(statuses))},
         "gpu_launches": st["batches"] * 2 + (st["completed"] * 11 if outputs & pa.PA_OUT_CSR else 0),
         "clocks": clk.summary(),
+    }
+    return fig, ok
+
+
+def run_served(args):
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    fig, ok = measure_served(args, args.rate, args.serve_seconds, args.serve_outputs, world, rank)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0 if ok else 1
+    line = {
+        "metric": "served edges/s with p50/p99 latency (continuous batching)",
+        "value": fig["edges_per_s"], "unit": "edges/s", "n_gpus": world, "steps": 1,
+        "warmup": args.warmup, "ms_per_step": fig["span_s"] * 1e3, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (generator parameters only)",
+        "config": {"workload": fig["workload"], "requests": fig["requests"],
+                   "budget_gb_per_gpu": fig["budget_gb_per_gpu"],
+                   "parallelism": f"requests round-robin over {world} servers (one per rank)"
+                   if world > 1 else "single", "output": fig["output"]},
+        "p50_ms": fig["p50_ms"], "p99_ms": fig["p99_ms"], "max_ms": fig["max_ms"],
+        "requests_per_s": fig["served_requests_per_s"],
+        "offered_requests_per_s": fig["offered_requests_per_s"],
+        "offered_edges_per_s": fig["offered_edges_per_s"], "all_ok": ok,
+        "server_stats_rank0": fig["server_stats_rank0"],
+        "statuses_rank0": fig["statuses_rank0"], "gpu_launches": fig["gpu_launches"],
+        "clocks": fig["clocks"],
     }
     print(json.dumps(line), flush=True)
     return 0 if ok else 1
@@ -821,6 +928,14 @@ def main():
     ap.add_argument("--serve-budget-gb", type=float, default=150.0, help="served: HBM budget")
     ap.add_argument("--serve-outputs", choices=["pairs", "csr", "both"], default="csr",
                     help="served: what each finished request keeps on the device")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default workload: skip the batched and served figures in its line")
+    ap.add_argument("--serve-window", type=float, default=2.0,
+                    help="default line: arrival window of the served run at --rate")
+    ap.add_argument("--sustain-rate", type=float, default=100.0,
+                    help="default line: a request rate the server sustains")
+    ap.add_argument("--sustain-seconds", type=float, default=5.0,
+                    help="default line: arrival window at --sustain-rate")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

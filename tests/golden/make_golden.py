@@ -168,11 +168,16 @@ def digest_fixtures():
 
 
 # Full-size configurations: (name, n, d, p, seed, seed_mode, model, with_csr).
+# The longest runs first: the pool works through the list in order.
 FULLSIZE_CASES = [
     ("c3_p0.5", 2 ** 30, 4, 0.5, 1234, orc.SEED_CLIQUE, orc.MODEL_COPY, True),
-    ("c2", 10 ** 8, 16, 0.5, 7, orc.SEED_CLIQUE, orc.MODEL_COPY, True),
     ("c3_p0", 2 ** 30, 4, 0.0, 1234, orc.SEED_CLIQUE, orc.MODEL_COPY, False),
+    ("c2", 10 ** 8, 16, 0.5, 7, orc.SEED_CLIQUE, orc.MODEL_COPY, True),
     ("sba_n2^30", 2 ** 30, 4, 0.0, 1234, orc.SEED_STAR_REF, orc.MODEL_BA, False),
+    # the benchmark's smaller workloads (CPU-runnable case and profiling sizes)
+    ("c1", 10 ** 5, 4, 0.5, 42, orc.SEED_CLIQUE, orc.MODEL_COPY, True),
+    ("c3s", 2 ** 25, 4, 0.5, 1234, orc.SEED_CLIQUE, orc.MODEL_COPY, True),
+    ("c3m", 2 ** 26, 4, 0.5, 1234, orc.SEED_CLIQUE, orc.MODEL_COPY, True),
 ]
 
 

@@ -1,18 +1,27 @@
 """The benchmark configurations at their full sizes, on the GPU.
 
-The oracle cannot run 4.3e9 edges in a test, but it does not have to for the
-first nodes: a node's slots depend only on its own draws and on earlier nodes,
-so the first N nodes of any graph are the whole graph of N nodes.  Each test
-therefore checks (1) a prefix of millions of nodes bit-exact against the
-oracle, (2) properties over the whole graph that hold for every correct output
--- row sources, targets below their source, distinct targets per row, the
-closure of p = 0 -- (3) a second generation gives the same checksum, and, for
+Whole-graph parity: the device digest (pa_digest) of the entire edge list --
+and, where the configuration builds one, of the CSR's rowptr and col -- must
+equal the oracle's digest of the same configuration
+(tests/golden/fullsize_digests.json, written by tests/golden/make_golden.py
+from orc_graph_digests, which generates the whole graph on the CPU).  The
+digest is position-keyed, so a single wrong id or two ids in swapped slots
+anywhere in the 4.3e9 edges changes it.
+
+Besides that, each test checks (1) a prefix of millions of nodes element by
+element against the oracle (a node depends only on earlier nodes, so the first
+N nodes are the graph of N nodes; this localises a failure that the digest only
+detects), (2) properties over the whole graph that hold for every correct
+output -- row sources, targets below their source, distinct targets per row,
+the closure of p = 0 -- (3) a second generation gives the same digest, and, for
 n = 2^30, (4) the degree distribution against the reference's own `-A scm`
 run (KS statistic and tail exponent; the exponent does not drift with n: the
 oracle gives 2.8395 at 10^6 and 2.8374 at 2^25 nodes).  The CSR of n = 10^8,
-d = 16 is checked by its invariants: every row strictly ascending (own targets
-below the row id, then in-neighbours above it), no self entry, row lengths
-equal to the degrees, and both directions of every edge present (hash sums)."""
+d = 16 is also checked by its invariants: every row strictly ascending (own
+targets below the row id, then in-neighbours above it), no self entry, row
+lengths equal to the degrees, and both directions of every edge present (hash
+sums)."""
+import json
 import os
 
 import numpy as np
@@ -74,6 +83,14 @@ def check_prefix(E, d, p, seed, mode, nodes):
     assert bad.size == 0, f"prefix mismatch at pair {bad[:5]}"
 
 
+def fixture(name):
+    """The oracle's whole-graph digests of one configuration."""
+    with open(os.path.join(GOLD, "fullsize_digests.json")) as f:
+        cases = {c["name"]: c for c in json.load(f)["cases"]}
+    c = cases[name]
+    return {k: tuple(int(x, 16) for x in c[k]) for k in ("pairs", "rowptr", "col") if k in c}
+
+
 def free():
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
@@ -83,6 +100,7 @@ def free():
 def test_c3_full_size(pa, cuda_ok, p):
     """n = 2^30, d = 4, int64, clique seed, Philox seed 1234: ~4.3e9 edges, 68.7 GB."""
     n, d, seed, mode = 2 ** 30, 4, 1234, pa.PA_SEED_CLIQUE
+    want = fixture("c3_p0.5" if p else "c3_p0")
     prm = pa.make_params(n, d, p, seed=seed, id_bits=64, seed_mode=mode)
     edges, scratch = pa.alloc_buffers(prm)
     E = edges[: pa.edge_count(prm)]
@@ -90,14 +108,17 @@ def test_c3_full_size(pa, cuda_ok, p):
     st = pa.finish(scratch)
     assert st.status == 0
     seed_edges = orc.seed_edge_count(d, orc.SEED_CLIQUE)
+    # whole graph against the oracle
+    assert pa.digest(E.reshape(-1)) == want["pairs"], "whole-graph digest differs from the oracle"
     # (1) the first 2^22 nodes (2^20 at p = 0, where every node retries more)
     check_prefix(E, d, p, seed, orc.SEED_CLIQUE, 2 ** 22 if p else 2 ** 20)
     # (2) every row; at p = 0 every target stays in the seed clique 0..d
-    h1 = check_rows(E, n, d, seed_edges, closure=d if p == 0 else None)
+    check_rows(E, n, d, seed_edges, closure=d if p == 0 else None)
     # (3) the same bits again
     pa.generate_into(prm, edges, scratch)
     assert pa.finish(scratch).status == 0
-    assert check_rows(E, n, d, seed_edges) == h1
+    assert pa.digest(E.reshape(-1)) == want["pairs"]
+    del scratch
     if p == 0.5:
         # (4) degrees against the reference's own n = 10^6 run of the same model
         deg = pa.degrees(prm, E)
@@ -111,7 +132,26 @@ def test_c3_full_size(pa, cuda_ok, p):
         assert abs(tail_alpha(mine) - tail_alpha(ref)) < ALPHA_TOL
         assert int(deg.sum().item()) == 2 * E.shape[0]
         del deg
-    del edges, scratch, E
+        free()
+        # the whole CSR (rowptr and col) against the oracle's
+        rowptr, col = pa.build_csr(prm, E)
+        assert pa.digest(rowptr) == want["rowptr"]
+        assert pa.digest(col) == want["col"]
+        del rowptr, col
+    del edges, E
+    free()
+
+
+def test_sba_full_size(pa, cuda_ok):
+    """The BA model (-A sba) at n = 2^30, d = 4, int64, star seed, Philox seed 1234."""
+    n, d, seed = 2 ** 30, 4, 1234
+    want = fixture("sba_n2^30")
+    prm = pa.make_params(n, d, 0.0, seed=seed, id_bits=64, seed_mode=pa.PA_SEED_STAR_REF,
+                         model=pa.PA_MODEL_BA)
+    E, st = pa.generate(prm)
+    assert st.status == 0
+    assert pa.digest(E.reshape(-1)) == want["pairs"], "whole-graph digest differs from the oracle"
+    del E
     free()
 
 
@@ -119,10 +159,12 @@ def test_c2_full_size_with_csr(pa, cuda_ok):
     """n = 10^8, d = 16, int64, clique seed, Philox seed 7: ~1.6e9 edges, then CSR."""
     n, d, p, seed = 10 ** 8, 16, 0.5, 7
     prm = pa.make_params(n, d, p, seed=seed, id_bits=64, seed_mode=pa.PA_SEED_CLIQUE)
+    want = fixture("c2")
     E, st = pa.generate(prm)
     assert st.status == 0
     m = E.shape[0]
     seed_edges = orc.seed_edge_count(d, orc.SEED_CLIQUE)
+    assert pa.digest(E.reshape(-1)) == want["pairs"], "whole-graph digest differs from the oracle"
     check_prefix(E, d, p, seed, orc.SEED_CLIQUE, 2 ** 20)
     edge_hash = check_rows(E, n, d, seed_edges)
     # seed edges are part of the graph too
@@ -134,6 +176,7 @@ def test_c2_full_size_with_csr(pa, cuda_ok):
     del E
     free()
     assert col.shape[0] == 2 * m
+    assert pa.digest(rowptr) == want["rowptr"] and pa.digest(col) == want["col"]
     assert int(rowptr[0].item()) == 0 and int(rowptr[-1].item()) == 2 * m
     assert torch.equal(rowptr[1:] - rowptr[:-1], deg)
     del deg

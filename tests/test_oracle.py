@@ -397,9 +397,14 @@ def test_fullsize_digest_fixture_is_complete():
     """The committed whole-graph digests of the benchmark configurations."""
     with open(os.path.join(GOLD, "fullsize_digests.json")) as f:
         cases = {c["name"]: c for c in json.load(f)["cases"]}
-    for name in ("c3_p0.5", "c3_p0", "c2"):
+    for name in ("c3_p0.5", "c3_p0", "c2", "sba_n2^30", "c1", "c3s", "c3m"):
         c = cases[name]
         assert c["edges"] == orc.edge_count(c["n"], c["d"], c["seed_mode"])
         assert len(c["pairs"]) == 2 and all(len(h) == 16 for h in c["pairs"])
-    for name in ("c3_p0.5", "c2"):
+    for name in ("c3_p0.5", "c2", "c1", "c3s", "c3m"):
         assert "rowptr" in cases[name] and "col" in cases[name]
+    # the smallest one recomputed here: the fixture is the oracle's output
+    c = cases["c1"]
+    dg = orc.graph_digests(c["n"], c["d"], c["p"], c["seed"], c["seed_mode"], c["model"], True)
+    for k in ("pairs", "rowptr", "col"):
+        assert [f"{x:016x}" for x in dg[k]] == c[k]

@@ -15,6 +15,13 @@
 //   4. out part: each generated row's d targets ranked in registers and stored;
 //      the seed rows' targets come from the (canonical) seed edges.
 // Items pack (v, u) in 8 bytes, so graphs of 2^32 nodes and more are refused.
+//
+// The sort reads the pairs twice and the items twice per pass: one histogram
+// kernel counts the digits of every pass while reading the pairs once, and each
+// pass is one kernel that keeps its tile's items in registers from the load to
+// the store, taking each digit's offset from the tiles before it by decoupled
+// look-back (Merrill and Garland's single-pass prefix scan, as in Adinets and
+// Merrill's one-sweep radix sort) instead of a per-pass histogram and scan.
 #include <algorithm>
 #include <type_traits>
 #include <vector>
@@ -26,125 +33,6 @@ namespace pa {
 namespace {
 
 constexpr uint32_t kFull = 0xffffffffu;
-constexpr uint32_t kScanThreads = 256;
-constexpr uint32_t kScanItems = 8;
-constexpr uint32_t kScanTile = kScanThreads * kScanItems;
-
-// ---------------------------------------------------------------------------
-// Exclusive scan of int64 with decoupled look-back.  Tile status word:
-// bits 62-63 = 0 (empty), 1 (aggregate), 2 (inclusive prefix); bits 0-61 value.
-// ---------------------------------------------------------------------------
-constexpr unsigned long long kStAgg = 1ull << 62, kStInc = 2ull << 62,
-                             kValMask = (1ull << 62) - 1;
-
-__device__ __forceinline__ unsigned long long ld_status(const unsigned long long *p)
-{
-    return ld_acquire_u64(p);
-}
-
-// Exclusive scan of in[0, n) into out[0, n) (in == out allowed: a tile reads its
-// items before it writes them and touches no other tile's items).
-__global__ void __launch_bounds__(kScanThreads) scan_kernel(const int64_t *in, int64_t *out,
-                                                            uint64_t n, unsigned long long *status,
-                                                            unsigned long long *tile_ctr,
-                                                            uint64_t spin_limit_ns, uint32_t *err)
-{
-    __shared__ unsigned long long s_tile;
-    __shared__ int64_t s_warp[kScanThreads / 32];
-    __shared__ int64_t s_prefix;
-    if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1ull);
-    __syncthreads();
-    const uint64_t tile = s_tile;
-    const uint64_t base = tile * kScanTile + (uint64_t)threadIdx.x * kScanItems;
-    int64_t v[kScanItems];
-    int64_t sum = 0;
-#pragma unroll
-    for (uint32_t i = 0; i < kScanItems; ++i) {
-        v[i] = base + i < n ? in[base + i] : 0;
-        sum += v[i];
-    }
-    // block-wide exclusive scan of per-thread sums
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    int64_t x = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int64_t y = __shfl_up_sync(kFull, x, o);
-        if (lane >= (uint32_t)o) x += y;
-    }
-    if (lane == 31) s_warp[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        int64_t w = lane < kScanThreads / 32 ? s_warp[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int64_t y = __shfl_up_sync(kFull, w, o);
-            if (lane >= (uint32_t)o) w += y;
-        }
-        if (lane < kScanThreads / 32) s_warp[lane] = w;   // inclusive per warp
-    }
-    __syncthreads();
-    const int64_t block_total = s_warp[kScanThreads / 32 - 1];
-    int64_t thread_excl = x - sum + (warp ? s_warp[warp - 1] : 0);
-
-    // look-back
-    if (warp == 0) {
-        int64_t prefix = 0;
-        if (tile == 0) {
-            if (lane == 0) {
-                st_release_u64(status, kStInc | (unsigned long long)block_total);
-            }
-        } else {
-            if (lane == 0) st_release_u64(status + tile, kStAgg | (unsigned long long)block_total);
-            int64_t pred = (int64_t)tile - 1;
-            const uint64_t t0 = globaltimer_ns();
-            bool failed = false;
-            while (true) {
-                // each lane inspects one predecessor, newest first
-                const int64_t t = pred - (int64_t)lane;
-                unsigned long long st = t >= 0 ? ld_status(status + t) : (kStInc);
-                const uint32_t empty = __ballot_sync(kFull, (st >> 62) == 0);
-                const uint32_t inc = __ballot_sync(kFull, (st >> 62) == 2);
-                // lanes before the first empty one are usable; stop at the first inclusive
-                const uint32_t stop_empty = empty ? (uint32_t)(__ffs(empty) - 1) : 32u;
-                const uint32_t stop_inc = inc ? (uint32_t)(__ffs(inc) - 1) : 32u;
-                if (stop_inc < stop_empty) {
-                    // sum lanes [0, stop_inc] (the inclusive one included)
-                    const int64_t contrib = lane <= stop_inc ? (int64_t)(st & kValMask) : 0;
-                    int64_t s = contrib;
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
-                    prefix += s;
-                    break;
-                }
-                if (stop_empty > 0) {
-                    const int64_t contrib = lane < stop_empty ? (int64_t)(st & kValMask) : 0;
-                    int64_t s = contrib;
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
-                    prefix += s;
-                    pred -= stop_empty;
-                    continue;
-                }
-                if (globaltimer_ns() - t0 > spin_limit_ns) { failed = true; break; }
-                __nanosleep(64);
-            }
-            if (failed) {
-                if (lane == 0) atomicCAS(err, 0u, (uint32_t)PA_ERR_SPIN_TIMEOUT);
-            } else if (lane == 0) {
-                st_release_u64(status + tile, kStInc | (unsigned long long)(prefix + block_total));
-            }
-        }
-        if (lane == 0) s_prefix = prefix;
-    }
-    __syncthreads();
-    int64_t run = s_prefix + thread_excl;
-#pragma unroll
-    for (uint32_t i = 0; i < kScanItems; ++i) {
-        if (base + i < n) out[base + i] = run;
-        run += v[i];
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Out parts.
 // ---------------------------------------------------------------------------
@@ -168,19 +56,31 @@ __global__ void out_part_kernel(const Id *E, const int64_t *rowptr, Id *col, uin
     const uint32_t g = lane / d, i = lane - g * d;
     const bool used = lane < G * d;
     const uint64_t rows = n - (d + 1);
-    for (uint64_t r0 = w0 * G; r0 < rows; r0 += warps * G) {
-        const uint64_t row = r0 + g;
-        const bool act = used && row < rows;
-        Id dst = 0;
-        if (act) dst = E[2 * (seed_edges + row * d + i) + 1];
-        uint32_t rank = 0;
-        for (uint32_t j = 0; j < d; ++j) {
-            const Id o = __shfl_sync(kFull, dst, (g * d + j) & 31u);
-            rank += (o < dst) ? 1u : 0u;
+    // U warp passes per step, their loads issued together
+    constexpr uint32_t U = 4;
+    for (uint64_t r0 = w0 * G * U; r0 < rows; r0 += warps * G * U) {
+        Id dst[U];
+        int64_t start[U];
+#pragma unroll
+        for (uint32_t q = 0; q < U; ++q) {
+            const uint64_t row = r0 + q * G + g;
+            const bool act = used && row < rows;
+            dst[q] = act ? E[2 * (seed_edges + row * d + i) + 1] : (Id)0;
+            start[q] = act ? rowptr[row + d + 1] : 0;
         }
-        if (act) {
-            const uint64_t pos = (uint64_t)rowptr[row + d + 1] + rank;
-            if (pos < col_len) col[pos] = dst;
+#pragma unroll
+        for (uint32_t q = 0; q < U; ++q) {
+            const uint64_t row = r0 + q * G + g;
+            const bool act = used && row < rows;
+            uint32_t rank = 0;
+            for (uint32_t j = 0; j < d; ++j) {
+                const Id o = __shfl_sync(kFull, dst[q], (g * d + j) & 31u);
+                rank += (o < dst[q]) ? 1u : 0u;
+            }
+            if (act) {
+                const uint64_t pos = (uint64_t)start[q] + rank;
+                if (pos < col_len) col[pos] = dst[q];
+            }
         }
     }
 }
@@ -208,20 +108,30 @@ __global__ void seed_out_kernel(const Id *E, uint64_t seed_edges, uint32_t d, ui
 // (number of items with key < x), read off the run boundaries.  No atomics on
 // the node range, no per-row sorting, no special path for hub rows.
 //
-// A pass sorts 8 or 9 key bits: a histogram kernel counts the digits of every
-// tile of 8192 items into a digit-major table, an exclusive scan of the table
-// gives each (digit, tile) its output offset, and the scatter kernel ranks every
-// item within its tile stably -- each of 16 warps walks its 512 items in order,
-// 32 at a time, with __match_any_sync for equal digits and 16-bit per-warp
-// counters in shared memory, then the warps' counts are prefixed per digit --
-// stages the tile in shared memory in digit order and writes each digit's run
-// contiguously.
+// A pass sorts 8 or 9 key bits.  Its kernel claims tiles of 8192 items in
+// order from a counter; a tile's 512 threads load 16 items each into
+// registers, rank them stably -- each of 16 warps walks its 512 items in
+// order, 32 at a time, with __match_any_sync for equal digits and 16-bit
+// per-warp counters in shared memory -- publish the tile's count of every
+// digit, and look back over the tiles before it (their counts, or the running
+// total the nearest finished one published) for each digit's global offset.
+// The tile is then staged in shared memory in digit order and every digit's
+// run is written contiguously.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kRadixThreads = 512, kRadixWarps = kRadixThreads / 32;
 constexpr uint32_t kRadixBuckets = 512;   // the widest digit: 9 bits
-constexpr uint32_t kRadixRounds = 16;   // items per lane per tile
+constexpr uint32_t kRadixRounds = 16;     // items per lane per tile
 constexpr uint32_t kRadixTile = kRadixThreads * kRadixRounds;
+constexpr uint32_t kMaxPasses = 4;
 constexpr unsigned long long kBadKey = 0xffffffffull;   // sorts after every node id
+
+// Look-back status word of (tile, digit): bits 63-62 kind (1 = the tile's own
+// count, 2 = the running total through the tile), bits 61-56 the pass's epoch
+// (a word of another pass reads as not yet published), bits 55-0 the value.
+constexpr unsigned long long kLbAgg = 1ull << 62, kLbInc = 2ull << 62;
+constexpr unsigned long long kLbValMask = (1ull << 56) - 1;
+constexpr uint32_t kLbEpochShift = 56;
+constexpr uint32_t kLbWindow = 8;   // predecessors read per look-back step
 
 // Item i of a pass.  The first pass reads the pairs (ids above the node range,
 // never produced by the generator, become kBadKey and raise an error).
@@ -242,158 +152,216 @@ __device__ __forceinline__ unsigned long long radix_item(const void *src, uint64
     }
 }
 
-template <typename Id, bool First, uint32_t DB>
-__global__ void __launch_bounds__(kRadixThreads) radix_hist_kernel(const void *src, uint64_t n_items,
-                                                                   uint32_t shift, uint64_t n,
-                                                                   int64_t *table, uint64_t n_tiles,
-                                                                   uint32_t *err)
+// Digit counts of every pass over all items (the pairs read once): per-block
+// shared counters, flushed with one global atomic per nonzero digit.  Equal
+// digits of a warp are combined first (the top digit of a power-law graph is
+// dominated by its hub nodes).
+template <typename Id, uint32_t DB>
+__global__ void __launch_bounds__(kRadixThreads) radix_hist_all_kernel(const Id *E, uint64_t n_items,
+                                                                       uint64_t n, uint32_t passes,
+                                                                       unsigned long long *hist,
+                                                                       uint32_t *err)
 {
     constexpr uint32_t NB = 1u << DB, MASK = NB - 1;
-    __shared__ uint32_t cnt[NB];
-    for (uint32_t b = threadIdx.x; b < NB; b += kRadixThreads) cnt[b] = 0;
+    __shared__ uint32_t cnt[kMaxPasses * NB];
+    for (uint32_t b = threadIdx.x; b < kMaxPasses * NB; b += kRadixThreads) cnt[b] = 0;
     __syncthreads();
-    const uint64_t t = blockIdx.x;
-    const uint64_t base = t * kRadixTile;
-    for (uint32_t r = 0; r < kRadixRounds; ++r) {
-        const uint64_t i = base + (uint64_t)r * kRadixThreads + threadIdx.x;
-        if (i < n_items) {
-            const unsigned long long it = radix_item<Id, First>(src, i, n, err);
-            atomicAdd(&cnt[(uint32_t)(it >> (32 + shift)) & MASK], 1u);
+    const uint32_t lane = threadIdx.x & 31u;
+    constexpr uint32_t U = 4;   // items per thread per step, loaded together
+    const uint64_t stride = (uint64_t)gridDim.x * kRadixThreads * U;
+    for (uint64_t base = (uint64_t)blockIdx.x * kRadixThreads * U; base < n_items; base += stride) {
+        uint32_t key[U];
+#pragma unroll
+        for (uint32_t j = 0; j < U; ++j) {
+            const uint64_t i = base + j * kRadixThreads + threadIdx.x;
+            key[j] = i < n_items ? (uint32_t)(radix_item<Id, true>(E, i, n, err) >> 32) : 0u;
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < U; ++j) {
+            const bool valid = base + j * kRadixThreads + threadIdx.x < n_items;
+            for (uint32_t q = 0; q < passes; ++q) {
+                const uint32_t dg = valid ? (key[j] >> (DB * q)) & MASK : NB + lane;
+                const uint32_t peers = __match_any_sync(kFull, dg);
+                if (valid && (__ffs(peers) - 1) == (int)lane)
+                    atomicAdd(&cnt[q * NB + dg], __popc(peers));
+            }
         }
     }
     __syncthreads();
-    for (uint32_t b = threadIdx.x; b < NB; b += kRadixThreads) table[(uint64_t)b * n_tiles + t] = cnt[b];
+    for (uint32_t b = threadIdx.x; b < passes * NB; b += kRadixThreads)
+        if (cnt[b]) atomicAdd(hist + b, (unsigned long long)cnt[b]);
 }
 
-// Dynamic shared memory of the scatter kernel: the tile's items in digit order,
-// then the per-warp counts, ranks and bases.
+// Exclusive prefix of each pass's digit counts: base[q*NB + b] = items whose
+// pass-q digit is below b.  One block, one thread per pass.
+template <uint32_t DB>
+__global__ void radix_base_kernel(const unsigned long long *hist, uint32_t passes,
+                                  unsigned long long *base)
+{
+    constexpr uint32_t NB = 1u << DB;
+    const uint32_t q = threadIdx.x;
+    if (q >= passes) return;
+    unsigned long long acc = 0;
+    for (uint32_t b = 0; b < NB; ++b) {
+        base[q * NB + b] = acc;
+        acc += hist[q * NB + b];
+    }
+}
+
+// Dynamic shared memory of the pass kernel: the tile in digit order, each
+// digit's global offset less its start within the tile, the per-warp digit
+// counts (then the warps' bases within the tile), the claimed tile.
 template <uint32_t NB>
 struct RadixSmem {
     unsigned long long stage[kRadixTile];
-    unsigned long long goff[NB];                  // global offset of the digit's run, less its
-                                                  // start within the tile
-    uint16_t wcnt[kRadixWarps][NB];               // per-warp digit counts, then the warp's base
-                                                  // within the tile (digit start included)
-    uint16_t lrank[kRadixTile];                   // rank within the warp's items of its digit
+    unsigned long long goff[NB];
+    uint16_t wcnt[kRadixWarps][NB];
+    uint32_t wsum[kRadixWarps];
+    unsigned long long tile;
 };
 
 template <typename Id, bool First, uint32_t DB>
-__global__ void __launch_bounds__(kRadixThreads, 2) radix_scatter_kernel(const void *src,
-                                                                      unsigned long long *dst,
-                                                                      uint64_t n_items, uint32_t shift,
-                                                                      uint64_t n, const int64_t *offs,
-                                                                      uint64_t n_tiles, uint32_t *err)
+__global__ void __launch_bounds__(kRadixThreads, 2) radix_pass_kernel(
+    const void *src, unsigned long long *dst, uint64_t n_items, uint32_t shift, uint64_t n,
+    const unsigned long long *digit_base, unsigned long long *status, uint32_t epoch,
+    unsigned long long *tile_ctr, uint64_t spin_limit_ns, uint32_t *err)
 {
     constexpr uint32_t NB = 1u << DB, MASK = NB - 1;
-    constexpr uint32_t PER = NB > kRadixThreads ? NB / kRadixThreads : 1;   // digits per thread
+    static_assert(NB <= kRadixThreads, "one digit per thread");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     RadixSmem<NB> &S = *reinterpret_cast<RadixSmem<NB> *>(smem_raw);
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
     const uint32_t lt = lanemask_lt();
     for (uint32_t w = 0; w < kRadixWarps; ++w)
-        for (uint32_t b = threadIdx.x; b < NB; b += kRadixThreads) S.wcnt[w][b] = 0;
+        for (uint32_t b = tid; b < NB; b += kRadixThreads) S.wcnt[w][b] = 0;
+    if (tid == 0) S.tile = atomicAdd(tile_ctr, 1ull);
     __syncthreads();
-    const uint64_t t = blockIdx.x;
+    const uint64_t t = S.tile;
     const uint64_t tb = t * kRadixTile;
     const uint32_t tcount = (uint32_t)min((uint64_t)kRadixTile, n_items - tb);
     const uint32_t wo = warp * (kRadixRounds * 32);
-    // 1. stable ranks within the warp's items (in order, 32 per round); the
-    // loads of kBatch rounds are issued together
-    constexpr uint32_t kBatch = 8;
-    for (uint32_t r0 = 0; r0 < kRadixRounds; r0 += kBatch) {
-        uint32_t dgs[kBatch];
+
+    // 1. the tile's items into registers, then stable ranks within the warp's
+    // items (in order, 32 per round); two ranks per register
+    unsigned long long its[kRadixRounds];
 #pragma unroll
-        for (uint32_t q = 0; q < kBatch; ++q) {
-            const uint32_t k = wo + (r0 + q) * 32 + lane;
-            dgs[q] = k < tcount
-                         ? (uint32_t)(radix_item<Id, First>(src, tb + k, n, err) >> (32 + shift)) & MASK
-                         : NB + lane;   // unique for lanes past the end
-        }
+    for (uint32_t r = 0; r < kRadixRounds; ++r) {
+        const uint32_t k = wo + r * 32 + lane;
+        its[r] = k < tcount ? radix_item<Id, First>(src, tb + k, n, err) : 0ull;
+    }
+    uint32_t rk[kRadixRounds / 2];
 #pragma unroll
-        for (uint32_t q = 0; q < kBatch; ++q) {
-            const uint32_t k = wo + (r0 + q) * 32 + lane;
-            const bool valid = k < tcount;
-            const uint32_t dg = dgs[q];
-            const uint32_t peers = __match_any_sync(kFull, dg);
-            const uint32_t leader = __ffs(peers) - 1;
-            uint32_t old = 0;
-            if (valid && lane == leader) {
-                old = S.wcnt[warp][dg];
-                S.wcnt[warp][dg] = (uint16_t)(old + __popc(peers));
-            }
-            old = __shfl_sync(kFull, old, leader);
-            if (valid) S.lrank[k] = (uint16_t)(old + __popc(peers & lt));
-            // the next round's leader for a digit may be another lane: order
-            // this round's counter stores before the next round's loads
-            __syncwarp();
+    for (uint32_t r = 0; r < kRadixRounds; ++r) {
+        const uint32_t k = wo + r * 32 + lane;
+        const bool valid = k < tcount;
+        const uint32_t dg = valid ? (uint32_t)(its[r] >> (32 + shift)) & MASK : NB + lane;
+        const uint32_t peers = __match_any_sync(kFull, dg);
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t old = 0;
+        if (valid && lane == leader) {
+            old = S.wcnt[warp][dg];
+            S.wcnt[warp][dg] = (uint16_t)(old + __popc(peers));
         }
+        old = __shfl_sync(kFull, old, leader);
+        const uint32_t rank = old + __popc(peers & lt);
+        if (r & 1) rk[r / 2] |= rank << 16;
+        else rk[r / 2] = rank;
+        // the next round's leader for a digit may be another lane: order this
+        // round's counter stores before the next round's loads
+        __syncwarp();
     }
     __syncthreads();
-    // 2. per digit (thread j owns digits j*PER .. j*PER+PER-1): warp bases in
-    // warp order, the digit's total, then the digits' starts within the tile,
-    // folded into the warp bases and the global offsets so that phases 3 and 4
-    // make one randomly indexed shared access each per item (shared memory, not
-    // DRAM, is what bounds this kernel)
-    uint32_t tot[PER];
-    uint32_t mine = 0;
-#pragma unroll
-    for (uint32_t q = 0; q < PER; ++q) {
-        const uint32_t dg = threadIdx.x * PER + q;
-        tot[q] = 0;
-        if (dg < NB) {
-            uint32_t acc = 0;
-            for (uint32_t w = 0; w < kRadixWarps; ++w) {
-                const uint32_t c = S.wcnt[w][dg];
-                S.wcnt[w][dg] = (uint16_t)acc;
-                acc += c;
-            }
-            tot[q] = acc;
-            S.goff[dg] = (unsigned long long)offs[(uint64_t)dg * n_tiles + t];
+
+    // 2. thread j owns digit j: its warps' bases in warp order and its count in
+    // the tile, published for the tiles after this one
+    uint32_t tot = 0;
+    if (tid < NB) {
+        for (uint32_t w = 0; w < kRadixWarps; ++w) {
+            const uint32_t c = S.wcnt[w][tid];
+            S.wcnt[w][tid] = (uint16_t)tot;
+            tot += c;
         }
-        mine += tot[q];
     }
-    uint32_t x = mine;
+    const unsigned long long ep = (unsigned long long)epoch << kLbEpochShift;
+    unsigned long long before = 0;   // this digit's items in the tiles before t
+    if (tid < NB) {
+        unsigned long long *mine = status + t * NB + tid;
+        if (t == 0) {
+            st_relaxed_u64(mine, kLbInc | ep | tot);
+        } else {
+            st_relaxed_u64(mine, kLbAgg | ep | tot);
+            // 3. look back: add the counts of earlier tiles until one of them
+            // carries its running total (bounded wait on tiles not yet ranked).
+            // kLbWindow predecessors are read at once: one at a time, the
+            // running totals would advance one tile per L2 round trip, far
+            // slower than tiles are ranked.
+            uint64_t p = t;   // tiles [p, t) are accounted for
+            const uint64_t t0 = globaltimer_ns();
+            bool done = false;
+            while (!done && p > 0) {
+                unsigned long long w[kLbWindow];
+#pragma unroll
+                for (uint32_t k = 0; k < kLbWindow; ++k)
+                    w[k] = k < p ? ld_relaxed_u64(status + (p - 1 - k) * NB + tid) : 0ull;
+                uint32_t used = 0;
+                bool waiting = false;
+#pragma unroll
+                for (uint32_t k = 0; k < kLbWindow; ++k) {
+                    if (done || waiting || k >= p) continue;
+                    const bool ready =
+                        (w[k] >> 62) != 0 && ((w[k] >> kLbEpochShift) & 63ull) == epoch;
+                    if (!ready) {
+                        waiting = true;
+                        continue;
+                    }
+                    before += w[k] & kLbValMask;
+                    ++used;
+                    if ((w[k] >> 62) == 2) done = true;
+                }
+                p -= used;
+                if (waiting && !done) {
+                    if (globaltimer_ns() - t0 > spin_limit_ns) {
+                        atomicCAS(err, 0u, (uint32_t)PA_ERR_SPIN_TIMEOUT);
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+            }
+            st_relaxed_u64(mine, kLbInc | ep | (before + tot));
+        }
+    }
+    // 4. digit starts within the tile (exclusive scan of the counts over digits)
+    uint32_t x = tot;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t y = __shfl_up_sync(kFull, x, o);
         if (lane >= (uint32_t)o) x += y;
     }
-    __shared__ uint32_t s_wsum[kRadixWarps];
-    if (lane == 31) s_wsum[warp] = x;
+    if (lane == 31) S.wsum[warp] = x;
     __syncthreads();
-    uint32_t run = x - mine;
-    for (uint32_t w = 0; w < warp; ++w) run += s_wsum[w];
-#pragma unroll
-    for (uint32_t q = 0; q < PER; ++q) {
-        const uint32_t dg = threadIdx.x * PER + q;
-        if (dg < NB) {
-            for (uint32_t w = 0; w < kRadixWarps; ++w)   // <= tile size: fits 16 bits
-                S.wcnt[w][dg] = (uint16_t)(S.wcnt[w][dg] + run);
-            S.goff[dg] -= run;    // the run's global start >= its start in the tile
-        }
-        run += tot[q];
+    uint32_t start = x - tot;
+    for (uint32_t w = 0; w < warp; ++w) start += S.wsum[w];
+    if (tid < NB) {
+        for (uint32_t w = 0; w < kRadixWarps; ++w)   // <= tile size: fits 16 bits
+            S.wcnt[w][tid] = (uint16_t)(S.wcnt[w][tid] + start);
+        // the digit's global start less its start in the tile (the tile's items
+        // of smaller digits are counted in digit_base, so this is >= 0)
+        S.goff[tid] = digit_base[tid] + before - start;
     }
     __syncthreads();
-    // 3. the tile's items into shared memory in digit order (read again, from L2)
-    for (uint32_t r0 = 0; r0 < kRadixRounds; r0 += kBatch) {
-        unsigned long long its[kBatch];
+    // 5. the tile into shared memory in digit order
 #pragma unroll
-        for (uint32_t q = 0; q < kBatch; ++q) {
-            const uint32_t k = wo + (r0 + q) * 32 + lane;
-            its[q] = k < tcount ? radix_item<Id, First>(src, tb + k, n, err) : 0ull;
-        }
-#pragma unroll
-        for (uint32_t q = 0; q < kBatch; ++q) {
-            const uint32_t k = wo + (r0 + q) * 32 + lane;
-            if (k < tcount) {
-                const uint32_t dg = (uint32_t)(its[q] >> (32 + shift)) & MASK;
-                S.stage[S.wcnt[warp][dg] + S.lrank[k]] = its[q];
-            }
+    for (uint32_t r = 0; r < kRadixRounds; ++r) {
+        const uint32_t k = wo + r * 32 + lane;
+        if (k < tcount) {
+            const uint32_t dg = (uint32_t)(its[r] >> (32 + shift)) & MASK;
+            const uint32_t rank = (rk[r / 2] >> ((r & 1) * 16)) & 0xffffu;
+            S.stage[S.wcnt[warp][dg] + rank] = its[r];
         }
     }
     __syncthreads();
-    // 4. out in digit runs: consecutive threads write consecutive addresses
-    for (uint32_t k = threadIdx.x; k < tcount; k += kRadixThreads) {
+    // 6. out in digit runs: consecutive threads write consecutive addresses
+    for (uint32_t k = tid; k < tcount; k += kRadixThreads) {
         const unsigned long long it = S.stage[k];
         const uint32_t dg = (uint32_t)(it >> (32 + shift)) & MASK;
         dst[S.goff[dg] + k] = it;
@@ -422,22 +390,40 @@ __global__ void seed_prefix_kernel(const uint32_t *seed_out, uint32_t d, int64_t
 // One pass over the sorted items: in part entry i (key v, value u) goes to
 // col[outprefix(v + 1) + i], and rowptr[x] = outprefix(x) + #items with key < x
 // is written for every x in (key(i-1), key(i)] (i = n_items closes the range up
-// to n; keys >= n -- only after an input error -- count as n).
+// to n; keys >= n -- only after an input error -- count as n).  A thread takes
+// four consecutive items with two 16-byte loads.
 template <typename Id>
 __global__ void in_sorted_kernel(const unsigned long long *items, uint64_t n_items, uint64_t n,
                                  uint32_t d, uint64_t seed_edges, const int64_t *seed_pre, Id *col,
                                  uint64_t col_len, int64_t *rowptr)
 {
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n_items; i += stride) {
-        const unsigned long long it = i < n_items ? items[i] : ~0ull;
-        const uint64_t v = i < n_items ? min((uint64_t)(it >> 32), n) : n;
-        const uint64_t lo = i > 0 ? min((uint64_t)(items[i - 1] >> 32), n) + 1 : 0;
-        for (uint64_t x = lo; x <= v && x <= n; ++x)
-            rowptr[x] = (int64_t)(outprefix(x, d, seed_edges, seed_pre) + i);
-        if (i < n_items && v < n) {
-            const uint64_t pos = outprefix(v + 1, d, seed_edges, seed_pre) + i;
-            if (pos < col_len) col[pos] = (Id)(it & 0xffffffffull);
+    constexpr uint32_t U = 4;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x * U;
+    for (uint64_t i0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * U; i0 <= n_items;
+         i0 += stride) {
+        unsigned long long it[U];
+        if (i0 + U <= n_items) {
+            const ulonglong2 a = reinterpret_cast<const ulonglong2 *>(items + i0)[0];
+            const ulonglong2 b = reinterpret_cast<const ulonglong2 *>(items + i0)[1];
+            it[0] = a.x; it[1] = a.y; it[2] = b.x; it[3] = b.y;
+        } else {
+#pragma unroll
+            for (uint32_t q = 0; q < U; ++q) it[q] = i0 + q < n_items ? items[i0 + q] : ~0ull;
+        }
+        uint64_t prev = i0 > 0 ? min((uint64_t)(items[i0 - 1] >> 32), n) : ~0ull;
+#pragma unroll
+        for (uint32_t q = 0; q < U; ++q) {
+            const uint64_t i = i0 + q;
+            if (i > n_items) break;
+            const uint64_t v = i < n_items ? min((uint64_t)(it[q] >> 32), n) : n;
+            const uint64_t lo = prev + 1;   // 0 for the first item (prev = ~0)
+            for (uint64_t x = lo; x <= v && x <= n; ++x)
+                rowptr[x] = (int64_t)(outprefix(x, d, seed_edges, seed_pre) + i);
+            if (i < n_items && v < n) {
+                const uint64_t pos = outprefix(v + 1, d, seed_edges, seed_pre) + i;
+                if (pos < col_len) col[pos] = (Id)(it[q] & 0xffffffffull);
+            }
+            prev = v;
         }
     }
 }
@@ -453,8 +439,8 @@ int grid_for(uint64_t items, uint32_t threads, uint32_t per_sm = 8)
 }
 
 struct CsrLayout {
-    uint64_t status_off, ctr_off, err_off, seed_out_off, seed_pre_off, items_off, table_off, total;
-    uint64_t n_tiles;   // scan tiles the status region holds
+    uint64_t items_off, status_off, hist_off, base_off, ctr_off, err_off, seed_out_off,
+        seed_pre_off, total;
     uint64_t r_tiles;   // radix tiles
 };
 
@@ -463,16 +449,16 @@ bool csr_supported(uint64_t n) { return n < (1ull << 32); }
 
 CsrLayout csr_layout(uint64_t n, uint32_t d, uint64_t n_edges)
 {
+    (void)n;
     auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
     CsrLayout L{};
     L.r_tiles = (n_edges + kRadixTile - 1) / kRadixTile;
-    const uint64_t scan_len = std::max<uint64_t>(kRadixBuckets * L.r_tiles, n + 1);
-    L.n_tiles = (scan_len + kScanTile - 1) / kScanTile;
     uint64_t o = 0;
     L.items_off = o;    o += al(8 * std::max<uint64_t>(n_edges, 1));
-    L.table_off = o;    o += al(8 * kRadixBuckets * std::max<uint64_t>(L.r_tiles, 1));
-    L.status_off = o;   o += al(8 * L.n_tiles);
-    L.ctr_off = o;      o += 256;
+    L.status_off = o;   o += al(8 * kRadixBuckets * std::max<uint64_t>(L.r_tiles, 1));
+    L.hist_off = o;     o += al(8 * kMaxPasses * kRadixBuckets);
+    L.base_off = o;     o += al(8 * kMaxPasses * kRadixBuckets);
+    L.ctr_off = o;      o += 256;   // one tile counter per pass
     L.err_off = o;      o += 256;
     L.seed_out_off = o; o += al(4 * (d + 1));
     L.seed_pre_off = o; o += al(8 * (d + 2));
@@ -480,53 +466,44 @@ CsrLayout csr_layout(uint64_t n, uint32_t d, uint64_t n_edges)
     return L;
 }
 
-// Exclusive scan of len items (reuses the scratch's tile-status region).
-int run_scan(const int64_t *in, int64_t *out, uint64_t len, unsigned char *scratch,
-             const CsrLayout &L, cudaStream_t s)
-{
-    const uint64_t tiles = (len + kScanTile - 1) / kScanTile;
-    if (tiles == 0) return PA_OK;
-    if (tiles > L.n_tiles) return PA_ERR_CAPACITY;
-    unsigned long long *status = (unsigned long long *)(scratch + L.status_off);
-    unsigned long long *ctr = (unsigned long long *)(scratch + L.ctr_off);
-    cudaError_t e = cudaMemsetAsync(status, 0, 8 * tiles, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(ctr, 0, 8, s);
-    if (e != cudaSuccess) return set_cuda_error(e);
-    scan_kernel<<<(unsigned)tiles, kScanThreads, 0, s>>>(in, out, len, status, ctr, 2000000000ull,
-                                                         (uint32_t *)(scratch + L.err_off));
-    e = cudaGetLastError();
-    return e == cudaSuccess ? PA_OK : set_cuda_error(e);
-}
-
-// One stable pass over DB key bits from `shift` (histogram, scan, scatter).
+// Every pass of the sort: the histogram of all passes' digits, their bases,
+// then one kernel per pass.  The last pass always lands in A.
 template <typename Id, uint32_t DB>
-int radix_pass(bool first, const void *src, unsigned long long *dst, uint64_t m, uint32_t shift,
-               uint64_t n, int64_t *table, unsigned char *scratch, const CsrLayout &L, uint32_t *err,
+int radix_sort(const Id *E, uint64_t m, uint64_t n, uint32_t passes, unsigned long long *A,
+               unsigned long long *B, unsigned char *scratch, const CsrLayout &L, uint32_t *err,
                cudaStream_t s)
 {
     constexpr uint32_t NB = 1u << DB;
-    const unsigned tiles = (unsigned)L.r_tiles;
+    unsigned long long *hist = (unsigned long long *)(scratch + L.hist_off);
+    unsigned long long *base = (unsigned long long *)(scratch + L.base_off);
+    unsigned long long *ctr = (unsigned long long *)(scratch + L.ctr_off);
+    unsigned long long *status = (unsigned long long *)(scratch + L.status_off);
     const size_t smem = sizeof(RadixSmem<NB>);
-    cudaError_t e = cudaFuncSetAttribute(radix_scatter_kernel<Id, true, DB>,
+    cudaError_t e = cudaFuncSetAttribute(radix_pass_kernel<Id, true, DB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(radix_scatter_kernel<Id, false, DB>,
+        e = cudaFuncSetAttribute(radix_pass_kernel<Id, false, DB>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // status words of an earlier call must not read as this call's
+    if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, 8 * (uint64_t)NB * L.r_tiles, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(hist, 0, 8 * kMaxPasses * kRadixBuckets, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctr, 0, 8 * kMaxPasses, s);
     if (e != cudaSuccess) return set_cuda_error(e);
-    if (first)
-        radix_hist_kernel<Id, true, DB><<<tiles, kRadixThreads, 0, s>>>(src, m, shift, n, table,
-                                                                        L.r_tiles, err);
-    else
-        radix_hist_kernel<Id, false, DB><<<tiles, kRadixThreads, 0, s>>>(src, m, shift, n, table,
-                                                                         L.r_tiles, err);
-    const int rc = run_scan(table, table, (uint64_t)NB * L.r_tiles, scratch, L, s);
-    if (rc != PA_OK) return rc;
-    if (first)
-        radix_scatter_kernel<Id, true, DB><<<tiles, kRadixThreads, smem, s>>>(src, dst, m, shift, n,
-                                                                              table, L.r_tiles, err);
-    else
-        radix_scatter_kernel<Id, false, DB><<<tiles, kRadixThreads, smem, s>>>(src, dst, m, shift, n,
-                                                                               table, L.r_tiles, err);
+    radix_hist_all_kernel<Id, DB><<<grid_for(m / 4 + 1, kRadixThreads, 2), kRadixThreads, 0, s>>>(
+        E, m, n, passes, hist, err);
+    radix_base_kernel<DB><<<1, 32, 0, s>>>(hist, passes, base);
+    const unsigned tiles = (unsigned)L.r_tiles;
+    for (uint32_t q = 0; q < passes; ++q) {
+        const uint32_t shift = DB * q;
+        unsigned long long *dst = ((passes - 1 - q) % 2 == 0) ? A : B;
+        const void *src = q == 0 ? (const void *)E : (const void *)(((passes - q) % 2 == 0) ? A : B);
+        if (q == 0)
+            radix_pass_kernel<Id, true, DB><<<tiles, kRadixThreads, smem, s>>>(
+                src, dst, m, shift, n, base + q * NB, status, q + 1, ctr + q, 2000000000ull, err);
+        else
+            radix_pass_kernel<Id, false, DB><<<tiles, kRadixThreads, smem, s>>>(
+                src, dst, m, shift, n, base + q * NB, status, q + 1, ctr + q, 2000000000ull, err);
+    }
     e = cudaGetLastError();
     return e == cudaSuccess ? PA_OK : set_cuda_error(e);
 }
@@ -542,7 +519,6 @@ int csr_enqueue_t(const pa_params *prm, const GenPlan &p, const Id *E, int64_t *
     uint32_t *seed_out = (uint32_t *)(scratch + L.seed_out_off);
     int64_t *seed_pre = (int64_t *)(scratch + L.seed_pre_off);
     uint32_t *err = (uint32_t *)(scratch + L.err_off);
-    int64_t *table = (int64_t *)(scratch + L.table_off);
     unsigned long long *A = (unsigned long long *)(scratch + L.items_off);
     // the column buffer (>= 8 bytes per pair) holds the other ping-pong array
     // while sorting; the last pass always lands in A
@@ -556,20 +532,16 @@ int csr_enqueue_t(const pa_params *prm, const GenPlan &p, const Id *E, int64_t *
     // 9-bit digits when three passes cover the key (n < 2^27), else 8-bit ones
     const uint32_t db = bits <= 27 ? 9u : 8u;
     const uint32_t passes = (bits + db - 1) / db;
-    int rc = PA_OK;
-    for (uint32_t q = 0; q < passes && m > 0; ++q) {
-        const uint32_t shift = db * q;
-        unsigned long long *dst = ((passes - 1 - q) % 2 == 0) ? A : B;
-        const void *src = q == 0 ? (const void *)E : (const void *)(((passes - q) % 2 == 0) ? A : B);
-        rc = db == 9 ? radix_pass<Id, 9>(q == 0, src, dst, m, shift, n, table, scratch, L, err, s)
-                     : radix_pass<Id, 8>(q == 0, src, dst, m, shift, n, table, scratch, L, err, s);
+    if (m > 0) {
+        const int rc = db == 9 ? radix_sort<Id, 9>(E, m, n, passes, A, B, scratch, L, err, s)
+                               : radix_sort<Id, 8>(E, m, n, passes, A, B, scratch, L, err, s);
         if (rc != PA_OK) return rc;
     }
     const uint64_t col_len = 2 * m;
-    in_sorted_kernel<Id><<<grid_for(m + 1, 256), 256, 0, s>>>(A, m, n, d, p.seed_edges, seed_pre, col,
-                                                              col_len, rowptr);
-    out_part_kernel<Id><<<grid_for(n * d, 256), 256, 0, s>>>(E, rowptr, col, n, d, p.seed_edges,
-                                                             col_len);
+    in_sorted_kernel<Id><<<grid_for((m + 4) / 4, 256), 256, 0, s>>>(A, m, n, d, p.seed_edges,
+                                                                    seed_pre, col, col_len, rowptr);
+    out_part_kernel<Id><<<grid_for(n * d / 4 + 1, 256), 256, 0, s>>>(E, rowptr, col, n, d,
+                                                                     p.seed_edges, col_len);
     e = cudaGetLastError();
     return e == cudaSuccess ? PA_OK : set_cuda_error(e);
 }

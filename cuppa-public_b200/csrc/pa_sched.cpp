@@ -7,6 +7,10 @@
 // the scan stops there and the budget that frees up goes to it first.  Budget
 // comes back when a request (or part of it, e.g. its generation scratch once
 // the batch has run) is released.
+//
+// The request server tags each request with a lane (bulk or express) and
+// admits per lane: a scan for some lanes skips the others' requests, and an
+// aged request stops admission of its own lane only.
 #include <cstdint>
 #include <deque>
 #include <mutex>
@@ -14,10 +18,12 @@
 #include <unordered_map>
 
 #include "cuppa_pa.h"
+#include "pa_sched.h"
 
 struct pa_sched {
     struct Item {
         uint64_t ticket, bytes, t_submit;
+        uint32_t lane;
     };
     std::deque<Item> queue;
     std::unordered_map<uint64_t, uint64_t> held;   // admitted ticket -> bytes still held
@@ -25,6 +31,49 @@ struct pa_sched {
     uint32_t max_queue = 0;
     mutable std::mutex mu;
 };
+
+namespace pa {
+
+int sched_submit_lane(pa_sched *q, uint64_t ticket, uint64_t bytes, uint64_t now_ns, uint32_t lane)
+{
+    if (!q || lane >= 32) return PA_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(q->mu);
+    if (bytes > q->budget) return PA_ERR_CAPACITY;
+    if (q->max_queue && q->queue.size() >= q->max_queue) return PA_ERR_BUSY;
+    if (q->held.count(ticket)) return PA_ERR_INVALID;
+    for (const auto &it : q->queue)
+        if (it.ticket == ticket) return PA_ERR_INVALID;
+    q->queue.push_back({ticket, bytes, now_ns, lane});
+    return PA_OK;
+}
+
+uint32_t sched_admit_lanes(pa_sched *q, uint64_t now_ns, uint64_t *out, uint32_t cap,
+                           uint32_t lane_mask)
+{
+    if (!q || !out || cap == 0) return 0;
+    std::lock_guard<std::mutex> lk(q->mu);
+    uint32_t n = 0;
+    uint32_t open = lane_mask;   // lanes still admitting in this scan
+    for (auto it = q->queue.begin(); it != q->queue.end() && n < cap && open;) {
+        const uint32_t bit = 1u << it->lane;
+        if (!(open & bit)) {
+            ++it;
+        } else if (it->bytes <= q->budget - q->in_use) {
+            q->in_use += it->bytes;
+            q->held[it->ticket] = it->bytes;
+            out[n++] = it->ticket;
+            it = q->queue.erase(it);
+        } else if (now_ns - it->t_submit >= q->aging) {
+            open &= ~bit;   // an aged request keeps its turn in its lane
+            ++it;
+        } else {
+            ++it;
+        }
+    }
+    return n;
+}
+
+}  // namespace pa
 
 extern "C" {
 
@@ -42,35 +91,12 @@ void pa_sched_destroy(pa_sched *q) { delete q; }
 
 int pa_sched_submit(pa_sched *q, uint64_t ticket, uint64_t bytes, uint64_t now_ns)
 {
-    if (!q) return PA_ERR_INVALID;
-    std::lock_guard<std::mutex> lk(q->mu);
-    if (bytes > q->budget) return PA_ERR_CAPACITY;
-    if (q->max_queue && q->queue.size() >= q->max_queue) return PA_ERR_BUSY;
-    if (q->held.count(ticket)) return PA_ERR_INVALID;
-    for (const auto &it : q->queue)
-        if (it.ticket == ticket) return PA_ERR_INVALID;
-    q->queue.push_back({ticket, bytes, now_ns});
-    return PA_OK;
+    return pa::sched_submit_lane(q, ticket, bytes, now_ns, 0);
 }
 
 uint32_t pa_sched_admit(pa_sched *q, uint64_t now_ns, uint64_t *out, uint32_t cap)
 {
-    if (!q || !out || cap == 0) return 0;
-    std::lock_guard<std::mutex> lk(q->mu);
-    uint32_t n = 0;
-    for (auto it = q->queue.begin(); it != q->queue.end() && n < cap;) {
-        if (it->bytes <= q->budget - q->in_use) {
-            q->in_use += it->bytes;
-            q->held[it->ticket] = it->bytes;
-            out[n++] = it->ticket;
-            it = q->queue.erase(it);
-        } else if (now_ns - it->t_submit >= q->aging) {
-            break;   // an aged request keeps its turn
-        } else {
-            ++it;
-        }
-    }
-    return n;
+    return pa::sched_admit_lanes(q, now_ns, out, cap, ~0u);
 }
 
 int pa_sched_release(pa_sched *q, uint64_t ticket, uint64_t bytes)

@@ -122,7 +122,7 @@ class PaServerConfig(ctypes.Structure):
         ("ttl_ns", ctypes.c_uint64),
         ("aging_ns", ctypes.c_uint64),
         ("outputs", ctypes.c_uint32),
-        ("reserved0", ctypes.c_uint32),
+        ("express_edges", ctypes.c_uint32),
     ]
 
 
@@ -446,11 +446,14 @@ def digest(ids, index_base: int = 0, stream=None) -> tuple[int, int]:
     torch = _torch()
     if ids.dtype not in (torch.int32, torch.int64) or not ids.is_contiguous():
         raise ValueError("digest needs a contiguous int32 or int64 tensor")
-    acc = torch.zeros(2, dtype=torch.int64, device=ids.device)
+    s = stream if stream is not None else torch.cuda.current_stream()
+    with torch.cuda.stream(s):            # the accumulator is cleared on the launch stream
+        acc = torch.zeros(2, dtype=torch.int64, device=ids.device)
     check(lib().pa_digest(ctypes.c_void_p(ids.data_ptr()), ids.numel(),
                           32 if ids.dtype == torch.int32 else 64, index_base,
-                          ctypes.c_void_p(acc.data_ptr()), ctypes.c_void_p(_stream_ptr(stream))),
+                          ctypes.c_void_p(acc.data_ptr()), ctypes.c_void_p(int(s.cuda_stream))),
           "pa_digest")
+    s.synchronize()
     a, b = acc.tolist()
     return a & (2 ** 64 - 1), b & (2 ** 64 - 1)
 
@@ -739,12 +742,12 @@ class Server:
 
     def __init__(self, budget_bytes: int = 0, max_batch: int = 0, max_inflight: int = 0,
                  max_queue: int = 0, device: int = -1, ttl_ns: int = 0, aging_ns: int = 0,
-                 outputs: int = 0):
+                 outputs: int = 0, express_edges: int = 0):
         cfg = PaServerConfig()
         check(lib().pa_server_config_init(ctypes.byref(cfg)), "pa_server_config_init")
         cfg.budget_bytes, cfg.max_batch, cfg.max_inflight = budget_bytes, max_batch, max_inflight
         cfg.max_queue, cfg.device, cfg.ttl_ns, cfg.aging_ns = max_queue, device, ttl_ns, aging_ns
-        cfg.outputs = outputs
+        cfg.outputs, cfg.express_edges = outputs, express_edges
         h = ctypes.c_void_p()
         check(lib().pa_server_create(ctypes.byref(cfg), ctypes.byref(h)), "pa_server_create")
         self._h = h

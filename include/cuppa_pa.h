@@ -248,15 +248,20 @@ int pa_batch_generate(const pa_params *prms, uint32_t count, void *const *d_edge
 /* ---- request server ------------------------------------------------------------ */
 /* A served stream of independent generation requests (no counterpart in the
  * reference, which makes one graph per process run, src/main.cu:105-116).  One
- * control thread per server owns a CUDA stream on its device: it admits queued
- * requests while their device memory (edge buffer + generation scratch) fits
- * the budget, launches everything admitted as one batch (pa_batch_generate's
- * launches) whenever fewer than max_inflight batches are on the GPU -- so
- * requests that arrive while a batch runs form the next one -- and marks each
- * request done when its batch's completion event has fired.  A result stays in
- * device memory, owned by the server, until pa_server_release (or until it has
- * been finished for ttl_ns).  Submit, poll, wait and release may be called from
- * any thread. */
+ * control thread per server owns its CUDA streams on its device: it admits
+ * queued requests while their device memory (edge buffer + generation scratch)
+ * fits the budget, launches everything admitted as one batch
+ * (pa_batch_generate's launches) whenever a lane has fewer than max_inflight
+ * batches on the GPU -- so requests that arrive while a batch runs form the
+ * next one -- and marks each request done when its batch's completion event
+ * has fired; it never waits on the GPU.  Two lanes share the budget: requests
+ * of at most express_edges edges run in the express lane, on streams of the
+ * device's highest priority, so a small request that arrives while a large
+ * batch runs starts at that batch's next kernel boundary; each lane has
+ * max_inflight streams, so a lane's next batch fills the previous one's tail.
+ * A result stays in device memory, owned by the server, until
+ * pa_server_release (or until it has been finished for ttl_ns).  Submit, poll,
+ * wait and release may be called from any thread. */
 typedef struct pa_server pa_server;
 
 /* pa_server_config.outputs: what a finished request keeps on the device (a
@@ -267,14 +272,16 @@ enum { PA_OUT_PAIRS = 1, PA_OUT_CSR = 2 };
 typedef struct pa_server_config {
     uint64_t budget_bytes;   /* device memory for admitted requests; 0 = 3/4 of free memory */
     uint32_t max_batch;      /* requests per launch; 0 = 4096                              */
-    uint32_t max_inflight;   /* batches queued on the GPU at once; 0 = 2                   */
+    uint32_t max_inflight;   /* batches on the GPU at once per lane (each on its own
+                                stream); 0 = 2                                             */
     uint32_t max_queue;      /* queued (not yet admitted) requests; 0 = unlimited          */
     int32_t device;          /* CUDA device; -1 = the caller's current device              */
     uint64_t ttl_ns;         /* finished results unreleased this long are freed; 0 = never */
     uint64_t aging_ns;       /* a queued request that has waited this long is not passed
                                 over by smaller ones; 0 = 100 ms                           */
     uint32_t outputs;        /* PA_OUT_* mask; 0 = PA_OUT_PAIRS                            */
-    uint32_t reserved0;      /* must be 0                                                  */
+    uint32_t express_edges;  /* requests of at most this many edges use the express lane;
+                                0 = 2^22                                                   */
 } pa_server_config;
 
 typedef struct pa_result {

@@ -154,3 +154,42 @@ def test_csr_outputs_equal_alone(pa, cuda_ok, outputs):
             assert srv.release(t) == 0
         _drain(srv)
         assert srv.stats().bytes_in_use == 0
+
+
+def test_small_request_overtakes_a_running_large_batch(pa, cuda_ok):
+    """A small request submitted while a large batch runs goes to the express
+    lane (its own high-priority stream) and finishes before that batch: with
+    CSR outputs the large batch is a generation followed by a chain of CSR
+    kernels, and the small request's kernels take the SMs at the first kernel
+    boundary.  Both results equal the requests generated alone."""
+    out = pa.PA_OUT_CSR | pa.PA_OUT_PAIRS
+    big = pa.make_params(30_000_000, 16, 0.5, seed=11, id_bits=32)
+    small = pa.make_params(20_000, 4, 0.5, seed=12)
+    with pa.Server(budget_bytes=24 << 30, outputs=out) as srv:
+        # warm both lanes up (first launches load kernels)
+        for q in (pa.make_params(3_000_000, 16, 0.5, seed=1), small):
+            t = srv.submit(q)
+            assert srv.wait(t)[0] == 0
+            srv.release(t)
+        tb = srv.submit(big)
+        deadline = time.time() + 10
+        while srv.stats().running == 0 and time.time() < deadline:
+            time.sleep(0.0002)
+        time.sleep(0.002)                      # the large batch is on the GPU
+        ts = srv.submit(small)
+        rc_s, rs = srv.wait(ts)
+        rc_b, rb = srv.wait(tb)
+        assert rc_s == 0 and rc_b == 0 and rs.status == 0 and rb.status == 0
+        assert rs.t_submit_ns > rb.t_start_ns          # submitted while the batch ran
+        assert rs.t_done_ns < rb.t_done_ns, (rs.t_done_ns, rb.t_done_ns)
+        for q, res in ((small, rs), (big, rb)):
+            want_e, _ = pa.generate(q)
+            assert torch.equal(pa.Server.edges_view(res, q.id_bits), want_e)
+            want_rp, want_col = pa.build_csr(q, want_e)
+            rp, col = pa.Server.csr_view(res, q.n, q.id_bits)
+            assert torch.equal(rp, want_rp) and torch.equal(col, want_col)
+            del want_e, want_rp, want_col
+        srv.release(ts)
+        srv.release(tb)
+        _drain(srv)
+        assert srv.stats().bytes_in_use == 0

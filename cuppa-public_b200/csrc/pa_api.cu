@@ -10,6 +10,7 @@
 #include <cstring>
 
 #include "pa_internal.h"
+#include "pa_wide.h"
 
 namespace pa {
 
@@ -45,12 +46,14 @@ int make_plan(const pa_params *prm, GenPlan *plan)
     if (rc != PA_OK) return rc;
     GenPlan p{};
     p.id_bytes = prm->id_bits / 8;
-    p.groups = 32u / prm->d;
+    p.wide = prm->d > 32;
+    // d > 32: one node per warp (pa_wide.cu); the tile geometry below is unused
+    p.groups = p.wide ? 1u : 32u / prm->d;
     p.passes = prm->tile_passes ? prm->tile_passes : 2u;
     p.tile_nodes = p.groups * p.passes;
     p.u_first = (uint64_t)prm->d + 1;
     const uint64_t n_gen = prm->n - p.u_first;
-    p.n_tiles = (n_gen + p.tile_nodes - 1) / p.tile_nodes;
+    p.n_tiles = p.wide ? 0 : (n_gen + p.tile_nodes - 1) / p.tile_nodes;
     p.seed_edges = pa_seed_edge_count(prm->d, prm->seed_mode);
     p.n_edges = p.seed_edges + n_gen * prm->d;
     p.pth = p_threshold(prm->p);
@@ -65,9 +68,10 @@ int make_plan(const pa_params *prm, GenPlan *plan)
     const uint64_t want = prm->start_nodes == PA_START_NONE ? 0
                           : prm->start_nodes ? prm->start_nodes
                                              : kStartNodesAuto;
-    p.u_split = start_split(prm->n, p.u_first, (uint64_t)kSbTiles * p.tile_nodes, want);
+    p.u_split = p.wide ? prm->n
+                       : start_split(prm->n, p.u_first, (uint64_t)kSbTiles * p.tile_nodes, want);
     const uint64_t st_nodes = (uint64_t)kStartPasses * p.groups;
-    p.start_tiles = (p.u_split - p.u_first + st_nodes - 1) / st_nodes;
+    p.start_tiles = p.wide ? 0 : (p.u_split - p.u_first + st_nodes - 1) / st_nodes;
     p.scratch_bytes = p.start_offset + kStartAreaBytes;
     p.claim_tiles = prm->claim_tiles ? prm->claim_tiles : kClaimTilesAuto;
     *plan = p;
@@ -119,7 +123,11 @@ int pa_params_init(pa_params *out)
 int pa_params_check(const pa_params *prm)
 {
     if (!prm) return PA_ERR_INVALID;
-    if (prm->d == 0 || prm->d > 32) return prm->d == 0 ? PA_ERR_INVALID : PA_ERR_NOT_SUPPORTED;
+    if (prm->d == 0) return PA_ERR_INVALID;
+    // d up to the reference's int16 EdgeIndexType (src/Common/DataTypes.h:11-28);
+    // d > 32 runs the wide kernel (pa_wide.cu), whose node ids are 31-bit
+    if (prm->d > gen::kWideMaxD) return PA_ERR_NOT_SUPPORTED;
+    if (prm->d > 32 && prm->n > (1ull << 31)) return PA_ERR_NOT_SUPPORTED;
     if (prm->id_bits != 32 && prm->id_bits != 64) return PA_ERR_INVALID;
     if (prm->n < (uint64_t)prm->d + 1) return PA_ERR_INVALID;
     if (prm->id_bits == 32 && prm->n > 0x7fffffffull) return PA_ERR_INVALID;
@@ -127,7 +135,7 @@ int pa_params_check(const pa_params *prm)
     if (!(prm->p >= 0.0 && prm->p <= 1.0)) return PA_ERR_INVALID;
     if (prm->seed_mode != PA_SEED_STAR_REF && prm->seed_mode != PA_SEED_CLIQUE) return PA_ERR_INVALID;
     if (prm->layout != PA_LAYOUT_PAIRS && prm->layout != PA_LAYOUT_SLOTS) return PA_ERR_NOT_SUPPORTED;
-    if (prm->layout == PA_LAYOUT_SLOTS &&
+    if (prm->layout == PA_LAYOUT_SLOTS && prm->d <= 32 &&
         (prm->start_nodes != 0 || prm->n - prm->d - 1 > kStartNodesAuto))
         return PA_ERR_NOT_SUPPORTED;
     if (prm->tile_passes != 0 && prm->tile_passes != 1 && prm->tile_passes != 2 &&

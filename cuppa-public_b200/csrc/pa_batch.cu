@@ -246,7 +246,7 @@ int batch_prepare(const pa_params *prms, uint32_t count, BatchJob &J)
         const int rc = make_plan(&q, &J.plans[i]);
         if (rc != PA_OK) return rc;
         const GenPlan &p = J.plans[i];
-        if (p.slots) return PA_ERR_NOT_SUPPORTED;
+        if (p.slots || p.wide) return PA_ERR_NOT_SUPPORTED;
         if (prms[i].id_bits != prms[0].id_bits) return PA_ERR_INVALID;
         if (prms[i].n + p.tile_nodes + 32 >= (1ull << 32)) return PA_ERR_NOT_SUPPORTED;
         if (prms[i].flags != 0) return PA_ERR_INVALID;

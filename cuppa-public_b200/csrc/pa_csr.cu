@@ -28,6 +28,7 @@
 
 #include "pa_device.cuh"
 #include "pa_internal.h"
+#include "pa_wide.h"
 
 namespace pa {
 namespace {
@@ -43,15 +44,17 @@ __global__ void out_part_kernel(const Id *E, const int64_t *rowptr, Id *col, uin
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
     const uint64_t w0 = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    // seed rows: canonical seed edges are grouped by src, ascending dst
+    // seed rows: the seed rows' out-edges go to targets 0, 1, ... in order in
+    // both seed graphs (CLIQUE row v: 0..v-1; STAR_REF row d: 0..d-1), so an
+    // edge's position in its row is its target
     for (uint64_t e = w0 * 32 + lane; e < seed_edges; e += warps * 32) {
-        const uint64_t u = (uint64_t)E[2 * e];
-        // position of this edge among u's seed out-edges
-        uint64_t first = e;
-        while (first > 0 && (uint64_t)E[2 * (first - 1)] == u) --first;
-        const uint64_t pos = (uint64_t)rowptr[u] + (e - first);
-        if (u < n && pos < col_len) col[pos] = E[2 * e + 1];
+        const uint64_t u = (uint64_t)E[2 * e], t = (uint64_t)E[2 * e + 1];
+        if (u < n && t < u) {
+            const uint64_t pos = (uint64_t)rowptr[u] + t;
+            if (pos < col_len) col[pos] = E[2 * e + 1];
+        }
     }
+    if (d > 32) return;   // generated rows of d > 32: csr_out_wide (pa_wide.cu)
     const uint32_t G = 32u / d;
     const uint32_t g = lane / d, i = lane - g * d;
     const bool used = lane < G * d;
@@ -85,15 +88,12 @@ __global__ void out_part_kernel(const Id *E, const int64_t *rowptr, Id *col, uin
     }
 }
 
-// Out-degree of each seed node (its canonical seed edges).
-template <typename Id>
-__global__ void seed_out_kernel(const Id *E, uint64_t seed_edges, uint32_t d, uint32_t *seed_out)
+// Out-degree of each seed node: CLIQUE row v holds v edges (to 0..v-1),
+// STAR_REF node d holds d (to 0..d-1).
+__global__ void seed_out_kernel(uint32_t d, uint32_t seed_mode, uint32_t *seed_out)
 {
-    for (uint32_t v = threadIdx.x; v <= d; v += blockDim.x) {
-        uint32_t c = 0;
-        for (uint64_t e = 0; e < seed_edges; ++e) c += (uint64_t)E[2 * e] == v;
-        seed_out[v] = c;
-    }
+    for (uint32_t v = threadIdx.x; v <= d; v += blockDim.x)
+        seed_out[v] = seed_mode == PA_SEED_CLIQUE ? v : (v == d ? d : 0u);
 }
 
 // ---------------------------------------------------------------------------
@@ -525,7 +525,7 @@ int csr_enqueue_t(const pa_params *prm, const GenPlan &p, const Id *E, int64_t *
     unsigned long long *B = reinterpret_cast<unsigned long long *>(col);
     cudaError_t e = cudaMemsetAsync(err, 0, 4, s);
     if (e != cudaSuccess) return set_cuda_error(e);
-    seed_out_kernel<Id><<<1, 64, 0, s>>>(E, p.seed_edges, d, seed_out);
+    seed_out_kernel<<<1, 256, 0, s>>>(d, prm->seed_mode, seed_out);
     seed_prefix_kernel<<<1, 32, 0, s>>>(seed_out, d, seed_pre);
     uint32_t bits = 1;
     while (bits < 32 && (n >> bits) != 0) ++bits;   // keys < n need bits(n) bits; kBadKey sorts last
@@ -542,6 +542,11 @@ int csr_enqueue_t(const pa_params *prm, const GenPlan &p, const Id *E, int64_t *
                                                                     seed_pre, col, col_len, rowptr);
     out_part_kernel<Id><<<grid_for(n * d / 4 + 1, 256), 256, 0, s>>>(E, rowptr, col, n, d,
                                                                      p.seed_edges, col_len);
+    if (p.wide) {
+        // the generated rows of d > 32 (out_part_kernel wrote the seed rows)
+        const int rc = gen::csr_out_wide(p.id_bytes, E, rowptr, col, n, d, p.seed_edges, col_len, s);
+        if (rc != PA_OK) return rc;
+    }
     e = cudaGetLastError();
     return e == cudaSuccess ? PA_OK : set_cuda_error(e);
 }
@@ -555,7 +560,8 @@ int csr_enqueue(const pa_params *prm, const void *d_edges, int64_t *d_rowptr, vo
     const int rc = make_plan(prm, &p);
     if (rc != PA_OK) return rc;
     if (!d_edges || !d_rowptr || !d_col || !d_scratch) return PA_ERR_INVALID;
-    if (!csr_supported(prm->n) || p.slots) return PA_ERR_NOT_SUPPORTED;
+    if (!csr_supported(prm->n) || p.slots || (p.wide && prm->d > gen::kWideRankMaxD))
+        return PA_ERR_NOT_SUPPORTED;
     if ((reinterpret_cast<uintptr_t>(d_col) & 15u) || (reinterpret_cast<uintptr_t>(d_scratch) & 15u))
         return PA_ERR_INVALID;
     const CsrLayout L = csr_layout(prm->n, prm->d, p.n_edges);
@@ -581,7 +587,8 @@ int pa_csr_bytes(const pa_params *prm, uint64_t *rowptr_bytes, uint64_t *col_byt
     const int rc = make_plan(prm, &p);
     if (rc != PA_OK) return rc;
     if (!rowptr_bytes || !col_bytes || !scratch_bytes) return PA_ERR_INVALID;
-    if (!csr_supported(prm->n) || p.slots) return PA_ERR_NOT_SUPPORTED;
+    if (!csr_supported(prm->n) || p.slots || (p.wide && prm->d > gen::kWideRankMaxD))
+        return PA_ERR_NOT_SUPPORTED;
     *rowptr_bytes = 8 * (prm->n + 1);
     *col_bytes = 2 * p.n_edges * p.id_bytes;
     *scratch_bytes = csr_layout(prm->n, prm->d, p.n_edges).total;

@@ -77,10 +77,14 @@ __device__ __forceinline__ void seed_edge_of(uint64_t e, uint32_t d, uint32_t mo
                                              uint64_t &dst)
 {
     if (mode == 1) {
-        uint64_t v = 1, base = 0;
-        while (base + v <= e) { base += v; ++v; }
+        // row v starts at v(v-1)/2: v = floor((1 + sqrt(1 + 8e)) / 2), with the
+        // rounding of the square root corrected in integers
+        uint64_t v = (uint64_t)((1.0 + sqrt(1.0 + 8.0 * (double)e)) * 0.5);
+        if (v < 1) v = 1;
+        while (v > 1 && v * (v - 1) / 2 > e) --v;
+        while ((v + 1) * v / 2 <= e) ++v;
         src = v;
-        dst = e - base;
+        dst = e - v * (v - 1) / 2;
     } else {
         src = d;
         dst = e;

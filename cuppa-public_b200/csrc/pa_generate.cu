@@ -54,6 +54,7 @@
 #include <cstring>
 
 #include "pa_gen_core.cuh"
+#include "pa_wide.h"
 
 namespace pa {
 
@@ -411,6 +412,22 @@ int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, vo
 
 
     const uint32_t blocks = blocks_override ? blocks_override : prm->blocks;
+    if (plan.wide) {
+        // every node by the wide kernel, its slots starting as all-ones
+        const uint64_t slot_bytes = (plan.slots ? 1ull : 2ull) * plan.id_bytes;
+        e = cudaMemsetAsync(reinterpret_cast<unsigned char *>(d_edges) + a.seed_edges * slot_bytes,
+                            0xff, (prm->n - plan.u_first) * prm->d * slot_bytes, stream);
+        if (e != cudaSuccess) return set_cuda_error(e);
+        a.start_end = prm->n;
+        if ((mrc = mark(1)) != PA_OK) return mrc;
+        const int rc = launch_wide(plan.id_bytes, plan.slots, a,
+                                   reinterpret_cast<unsigned long long *>(
+                                       reinterpret_cast<unsigned char *>(d_scratch) + plan.start_offset),
+                                   blocks, stream);
+        if (rc != PA_OK) return rc;
+        if ((mrc = mark(2)) != PA_OK) return mrc;
+        return mark(3);
+    }
     // 32-bit node arithmetic needs every node id, and tile base + tile_nodes,
     // below 2^32 - 32 (the top 32 values are the unknown-lane match keys).
     const bool small = prm->n + plan.tile_nodes + 32 < (1ull << 32);

@@ -67,6 +67,7 @@ struct GenPlan {
     uint64_t pth;           // direct threshold
     uint32_t model;         // PA_MODEL_*
     bool slots;             // PA_LAYOUT_SLOTS: targets only, seed rows implied
+    bool wide;              // d > 32: the wide kernel (pa_wide.cu) generates every node
     uint64_t edges_bytes;
     uint64_t scratch_bytes;
     uint64_t spin_limit_ns;

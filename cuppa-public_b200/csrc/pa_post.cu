@@ -3,6 +3,7 @@
 // copies the whole graph to the host and counts there).
 #include "pa_device.cuh"
 #include "pa_internal.h"
+#include "pa_wide.h"
 
 namespace pa {
 namespace {
@@ -177,6 +178,28 @@ __global__ void __launch_bounds__(256) digest_kernel(const Id *x, uint64_t count
     }
 }
 
+// The same for d > 32: one thread per slot (slot j of row j / d); the row's
+// node gets its d increments from the thread of the row's first slot.
+template <typename Id>
+__global__ void degree_slots_any_kernel(const Id *S, uint64_t rows, uint32_t d, uint64_t u_first,
+                                        uint32_t seed_mode, uint64_t seed_edges, uint64_t n,
+                                        unsigned long long *deg)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t t0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (uint64_t e = t0; e < seed_edges; e += stride) {
+        uint64_t s, t;
+        seed_edge_of(e, d, seed_mode, s, t);
+        atomicAdd(deg + s, 1ull);
+        atomicAdd(deg + t, 1ull);
+    }
+    for (uint64_t j = t0; j < rows * d; j += stride) {
+        const unsigned long long t = (unsigned long long)S[j];
+        if (t < n) atomicAdd(deg + t, 1ull);   // ids are used as addresses: never trust them
+        if (j % d == 0) atomicAdd(deg + u_first + j / d, (unsigned long long)d);
+    }
+}
+
 int grid_for(uint64_t work_items, uint32_t threads)
 {
     int dev = 0, sms = 148;
@@ -206,6 +229,7 @@ int pa_canonicalize(const pa_params *prm, const void *d_edges, void *d_out, void
     const uint32_t threads = 256;
     const int grid = grid_for(rows * prm->d, threads);
     cudaStream_t s = (cudaStream_t)stream;
+    if (p.wide) return gen::canon_wide(p.id_bytes, d_edges, d_out, prm->n, prm->d, p.seed_edges, s);
     if (p.id_bytes == 8)
         canon_kernel<int64_t><<<grid, threads, 0, s>>>((const int64_t *)d_edges, (int64_t *)d_out,
                                                        prm->n, prm->d, p.seed_edges);
@@ -227,7 +251,17 @@ int pa_degrees(const pa_params *prm, const void *d_edges, int64_t *d_deg, void *
     if (e != cudaSuccess) return set_cuda_error(e);
     const uint32_t threads = 256;
     const int grid = grid_for(p.n_edges, threads);
-    if (p.slots) {
+    if (p.slots && p.wide) {
+        const uint64_t rows = prm->n - p.u_first;
+        if (p.id_bytes == 8)
+            degree_slots_any_kernel<int64_t><<<grid, threads, 0, s>>>(
+                (const int64_t *)d_edges, rows, prm->d, p.u_first, prm->seed_mode, p.seed_edges,
+                prm->n, (unsigned long long *)d_deg);
+        else
+            degree_slots_any_kernel<int32_t><<<grid, threads, 0, s>>>(
+                (const int32_t *)d_edges, rows, prm->d, p.u_first, prm->seed_mode, p.seed_edges,
+                prm->n, (unsigned long long *)d_deg);
+    } else if (p.slots) {
         const uint64_t rows = prm->n - p.u_first;
         if (p.id_bytes == 8)
             degree_slots_kernel<int64_t><<<grid, threads, 0, s>>>(

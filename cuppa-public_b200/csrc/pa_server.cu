@@ -668,7 +668,7 @@ int pa_server_submit(pa_server *S, const pa_params *prm, uint64_t *ticket)
     int rc = make_plan(prm, &p);
     if (rc != PA_OK) return rc;
     if (prm->flags != 0) return PA_ERR_INVALID;
-    if (p.slots) return PA_ERR_NOT_SUPPORTED;
+    if (p.slots || p.wide) return PA_ERR_NOT_SUPPORTED;
     Request r;
     r.prm = *prm;
     r.n_edges = p.n_edges;

@@ -652,6 +652,7 @@ int pa_stream_edges(const pa_params *prm, const void *d_edges, int format, uint6
     GenPlan p;
     const int rc = make_plan(prm, &p);
     if (rc != PA_OK) return rc;
+    if (prm->d > kTileEdges) return PA_ERR_NOT_SUPPORTED;   // a tile holds one row at least
     if (!sink || (format != PA_FORMAT_TEXT && format != PA_FORMAT_BINARY)) return PA_ERR_INVALID;
     if (!d_edges && prm->n > p.u_first) return PA_ERR_INVALID;
     return stream_edges(prm, p, d_edges, format, chunk_edges, sink, ctx, (cudaStream_t)stream,

@@ -66,7 +66,10 @@ def test_param_checks(pa):
 
     assert rc() == pa.PA_OK
     assert rc(d=0) == pa.PA_ERR_INVALID
-    assert rc(d=33) == pa.PA_ERR_NOT_SUPPORTED
+    assert rc(d=33) == pa.PA_OK                        # the wide kernel (d > 32)
+    assert rc(d=32767, n=40000) == pa.PA_OK            # the reference's int16 EdgeIndexType
+    assert rc(d=32768, n=40000) == pa.PA_ERR_NOT_SUPPORTED
+    assert rc(d=33, n=2 ** 31 + 1, id_bits=64) == pa.PA_ERR_NOT_SUPPORTED   # 31-bit node ids
     assert rc(n=4, d=4) == pa.PA_ERR_INVALID          # fewer than d+1 nodes
     assert rc(n=5, d=4) == pa.PA_OK                   # the seed graph alone
     assert rc(p=-0.1) == pa.PA_ERR_INVALID

@@ -1,0 +1,124 @@
+"""Nodes with more than 32 edges (32 < d <= 32767, the reference's int16
+EdgeIndexType): the wide kernel against the oracle, bit-exact, with every slot
+value, its order and the retry count compared -- both id widths, both seed
+graphs, both layouts, the BA model, p from 0 to 1 -- and the post-processing of
+such graphs (canonical rows, degrees, CSR, digest, text) against the oracle's."""
+import numpy as np
+import pytest
+import torch
+
+import _oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+SWEEP = []
+for d in (33, 64, 100, 1000):
+    for bits in (32, 64):
+        SWEEP.append((max(4 * d, 3000), d, 0.5, 900 + d, 1, bits))
+for p in (0.0, 0.1, 0.9, 1.0):
+    SWEEP.append((2000, 48, p, 7, 1, 32))
+SWEEP += [(3000, 40, 0.5, 2 ** 40 + 3, 0, 64), (1200, 257, 0.3, 5, 0, 32), (5000, 33, 0.5, 1, 1, 32),
+          (34, 33, 0.5, 2, 1, 32), (100, 33, 0.0, 3, 0, 32)]
+
+
+def _check(pa, n, d, p, seed, mode, bits, **kw):
+    prm = pa.make_params(n, d, p, seed=seed, id_bits=bits, seed_mode=mode, **kw)
+    edges, st = pa.generate(prm)
+    assert st.status == 0
+    G, retries = orc.generate(n, d, p, seed, mode, with_retries=True)
+    want = orc.pairs_slot_order(G, mode)
+    got = edges.cpu().numpy().astype(np.int64)
+    bad = np.nonzero((got != want).any(axis=1))[0]
+    assert bad.size == 0, f"first mismatch at pair {bad[:5]}"
+    assert st.retries == retries
+    return prm, edges, G
+
+
+@pytest.mark.parametrize("n,d,p,seed,mode,bits", SWEEP)
+def test_wide_bit_exact(pa, cuda_ok, n, d, p, seed, mode, bits):
+    _check(pa, n, d, p, seed, mode, bits)
+
+
+@pytest.mark.parametrize("blocks", [1, 7, 300])
+def test_wide_any_grid(pa, cuda_ok, blocks):
+    """Any grid gives the same graph (claims in node order, bounded waits)."""
+    _check(pa, 4000, 70, 0.4, 11, 1, 32, blocks=blocks)
+
+
+def test_wide_large_d(pa, cuda_ok):
+    _check(pa, 8200, 8192, 0.5, 3, 1, 32)
+
+
+def test_wide_largest_d(pa, cuda_ok):
+    """d = 32767, the largest the reference's int16 slot index allows: three
+    generated nodes on a 32768-node clique (5.4e8 seed edges).  The oracle's
+    quadratic duplicate scan and its int64 slot array (8.6 GB) are too large at
+    this size, so the rows are checked by their properties and the seed edges by
+    their closed form; d = 8192 above is compared with the oracle."""
+    d = 32767
+    n = d + 4
+    prm = pa.make_params(n, d, 0.5, seed=3, id_bits=32)
+    E, st = pa.generate(prm)
+    assert st.status == 0
+    S = d * (d + 1) // 2
+    rows = E[S:].view(n - d - 1, d, 2).to(torch.int64)
+    u = torch.arange(d + 1, n, device=E.device)
+    assert bool((rows[:, :, 0] == u[:, None]).all())
+    v = rows[:, :, 1]
+    assert bool((v >= 0).all()) and bool((v < u[:, None]).all())
+    sv, _ = torch.sort(v, dim=1)
+    assert bool((sv[:, 1:] > sv[:, :-1]).all())
+    seed = E[:S].to(torch.int64)
+    src = torch.repeat_interleave(torch.arange(1, d + 1, device=E.device),
+                                  torch.arange(1, d + 1, device=E.device))
+    assert torch.equal(seed[:, 0], src)
+    starts = src * (src - 1) // 2
+    assert torch.equal(seed[:, 1], torch.arange(S, device=E.device) - starts)
+
+
+def test_wide_ba_and_slots(pa, cuda_ok):
+    n, d = 3000, 50
+    prm = pa.make_params(n, d, 0.0, seed=9, seed_mode=pa.PA_SEED_STAR_REF, model=pa.PA_MODEL_BA)
+    E, st = pa.generate(prm)
+    assert st.status == 0
+    G = orc.generate_ba(n, d, 9)
+    assert (E.cpu().numpy() == orc.pairs_slot_order(G, orc.SEED_STAR_REF)).all()
+    prm = pa.make_params(n, d, 0.5, seed=4, layout=pa.PA_LAYOUT_SLOTS, id_bits=64)
+    S, st = pa.generate(prm)
+    assert st.status == 0
+    G = orc.generate(n, d, 0.5, 4, orc.SEED_CLIQUE)
+    assert (S.cpu().numpy() == G[d + 1:]).all()
+    deg = pa.degrees(prm, S).cpu().numpy()
+    assert (deg == orc.degrees(G, orc.SEED_CLIQUE)).all()
+
+
+@pytest.mark.parametrize("d,bits", [(33, 32), (100, 64), (1000, 32)])
+def test_wide_post_processing(pa, cuda_ok, d, bits):
+    n, p, seed, mode = max(3 * d, 3000), 0.5, 21, 1
+    prm, E, G = _check(pa, n, d, p, seed, mode, bits)
+    assert pa.digest(E.reshape(-1)) == orc.digest_ids(orc.pairs_slot_order(G, mode))
+    assert (pa.degrees(prm, E).cpu().numpy() == orc.degrees(G, mode)).all()
+    rowptr, col = pa.build_csr(prm, E)
+    want_rp, want_col = orc.csr(G, mode)
+    assert (rowptr.cpu().numpy() == want_rp).all() and (col.cpu().numpy() == want_col).all()
+    out = torch.empty_like(E)
+    pa.canonicalize(prm, E, out)
+    assert (out.cpu().numpy() == orc.pairs_canonical(G, mode)).all()
+    pa.canonicalize(prm, E)          # in place
+    assert torch.equal(out, E)
+    parts = []
+    pa.stream_edges(prm, out, parts.append, chunk_edges=5000)
+    text = "".join(f"{u} {v}\n" for u, v in orc.pairs_canonical(G, mode).tolist())
+    assert b"".join(parts) == text.encode()
+
+
+def test_wide_limits(pa, cuda_ok):
+    prm = pa.make_params(40000, 5000, 0.5, seed=1)
+    E, st = pa.generate(prm)
+    assert st.status == 0
+    with pytest.raises(pa.CuppaError) as ei:
+        pa.build_csr(prm, E)                # rows above 4096 entries are not ranked
+    assert ei.value.status == pa.PA_ERR_NOT_SUPPORTED
+    with pa.Server(budget_bytes=1 << 30) as srv:
+        rc, _ = srv.try_submit(pa.make_params(1000, 40, 0.5))
+        assert rc == pa.PA_ERR_NOT_SUPPORTED

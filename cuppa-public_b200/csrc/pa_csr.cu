@@ -131,7 +131,7 @@ constexpr unsigned long long kBadKey = 0xffffffffull;   // sorts after every nod
 constexpr unsigned long long kLbAgg = 1ull << 62, kLbInc = 2ull << 62;
 constexpr unsigned long long kLbValMask = (1ull << 56) - 1;
 constexpr uint32_t kLbEpochShift = 56;
-constexpr uint32_t kLbWindow = 8;   // predecessors read per look-back step
+constexpr uint32_t kLbWindow = 4;   // predecessors read per look-back step
 
 // Item i of a pass.  The first pass reads the pairs (ids above the node range,
 // never produced by the generator, become kBadKey and raise an error).
@@ -153,9 +153,9 @@ __device__ __forceinline__ unsigned long long radix_item(const void *src, uint64
 }
 
 // Digit counts of every pass over all items (the pairs read once): per-block
-// shared counters, flushed with one global atomic per nonzero digit.  Equal
-// digits of a warp are combined first (the top digit of a power-law graph is
-// dominated by its hub nodes).
+// shared counters, flushed with one global atomic per nonzero digit.  (Combining
+// a warp's equal digits with __match_any_sync first measured far slower than
+// the shared atomics it saves: 32 against ~5 ms at n = 10^8, d = 16.)
 template <typename Id, uint32_t DB>
 __global__ void __launch_bounds__(kRadixThreads) radix_hist_all_kernel(const Id *E, uint64_t n_items,
                                                                        uint64_t n, uint32_t passes,
@@ -166,7 +166,6 @@ __global__ void __launch_bounds__(kRadixThreads) radix_hist_all_kernel(const Id 
     __shared__ uint32_t cnt[kMaxPasses * NB];
     for (uint32_t b = threadIdx.x; b < kMaxPasses * NB; b += kRadixThreads) cnt[b] = 0;
     __syncthreads();
-    const uint32_t lane = threadIdx.x & 31u;
     constexpr uint32_t U = 4;   // items per thread per step, loaded together
     const uint64_t stride = (uint64_t)gridDim.x * kRadixThreads * U;
     for (uint64_t base = (uint64_t)blockIdx.x * kRadixThreads * U; base < n_items; base += stride) {
@@ -178,13 +177,9 @@ __global__ void __launch_bounds__(kRadixThreads) radix_hist_all_kernel(const Id 
         }
 #pragma unroll
         for (uint32_t j = 0; j < U; ++j) {
-            const bool valid = base + j * kRadixThreads + threadIdx.x < n_items;
-            for (uint32_t q = 0; q < passes; ++q) {
-                const uint32_t dg = valid ? (key[j] >> (DB * q)) & MASK : NB + lane;
-                const uint32_t peers = __match_any_sync(kFull, dg);
-                if (valid && (__ffs(peers) - 1) == (int)lane)
-                    atomicAdd(&cnt[q * NB + dg], __popc(peers));
-            }
+            if (base + j * kRadixThreads + threadIdx.x >= n_items) continue;
+            for (uint32_t q = 0; q < passes; ++q)
+                atomicAdd(&cnt[q * NB + ((key[j] >> (DB * q)) & MASK)], 1u);
         }
     }
     __syncthreads();
@@ -241,20 +236,34 @@ __global__ void __launch_bounds__(kRadixThreads, 2) radix_pass_kernel(
     const uint32_t tcount = (uint32_t)min((uint64_t)kRadixTile, n_items - tb);
     const uint32_t wo = warp * (kRadixRounds * 32);
 
-    // 1. the tile's items into registers, then stable ranks within the warp's
-    // items (in order, 32 per round); two ranks per register
-    unsigned long long its[kRadixRounds];
+    // 1. the tile's items, loaded together, parked in the stage in their own
+    // order (conflict-free); only their digits stay in registers through the
+    // ranking and the look-back, which keeps the kernel free of spills
+    uint32_t dgp[kRadixRounds / 2];   // two digits per register
+    {
+        unsigned long long its[kRadixRounds];
 #pragma unroll
-    for (uint32_t r = 0; r < kRadixRounds; ++r) {
-        const uint32_t k = wo + r * 32 + lane;
-        its[r] = k < tcount ? radix_item<Id, First>(src, tb + k, n, err) : 0ull;
+        for (uint32_t r = 0; r < kRadixRounds; ++r) {
+            const uint32_t k = wo + r * 32 + lane;
+            its[r] = k < tcount ? radix_item<Id, First>(src, tb + k, n, err) : 0ull;
+        }
+#pragma unroll
+        for (uint32_t r = 0; r < kRadixRounds; ++r) {
+            const uint32_t k = wo + r * 32 + lane;
+            S.stage[k] = its[r];
+            const uint32_t dg = k < tcount ? (uint32_t)(its[r] >> (32 + shift)) & MASK : NB + lane;
+            if (r & 1) dgp[r / 2] |= dg << 16;
+            else dgp[r / 2] = dg;
+        }
     }
+    // stable ranks within the warp's items (in order, 32 per round); two ranks
+    // per register
     uint32_t rk[kRadixRounds / 2];
 #pragma unroll
     for (uint32_t r = 0; r < kRadixRounds; ++r) {
         const uint32_t k = wo + r * 32 + lane;
         const bool valid = k < tcount;
-        const uint32_t dg = valid ? (uint32_t)(its[r] >> (32 + shift)) & MASK : NB + lane;
+        const uint32_t dg = (dgp[r / 2] >> ((r & 1) * 16)) & 0xffffu;
         const uint32_t peers = __match_any_sync(kFull, dg);
         const uint32_t leader = __ffs(peers) - 1;
         uint32_t old = 0;
@@ -349,14 +358,20 @@ __global__ void __launch_bounds__(kRadixThreads, 2) radix_pass_kernel(
         S.goff[tid] = digit_base[tid] + before - start;
     }
     __syncthreads();
-    // 5. the tile into shared memory in digit order
+    // 5. the tile back from its parking place, then into the stage in digit order
+    {
+        unsigned long long its[kRadixRounds];
 #pragma unroll
-    for (uint32_t r = 0; r < kRadixRounds; ++r) {
-        const uint32_t k = wo + r * 32 + lane;
-        if (k < tcount) {
-            const uint32_t dg = (uint32_t)(its[r] >> (32 + shift)) & MASK;
-            const uint32_t rank = (rk[r / 2] >> ((r & 1) * 16)) & 0xffffu;
-            S.stage[S.wcnt[warp][dg] + rank] = its[r];
+        for (uint32_t r = 0; r < kRadixRounds; ++r) its[r] = S.stage[wo + r * 32 + lane];
+        __syncthreads();
+#pragma unroll
+        for (uint32_t r = 0; r < kRadixRounds; ++r) {
+            const uint32_t k = wo + r * 32 + lane;
+            if (k < tcount) {
+                const uint32_t dg = (dgp[r / 2] >> ((r & 1) * 16)) & 0xffffu;
+                const uint32_t rank = (rk[r / 2] >> ((r & 1) * 16)) & 0xffffu;
+                S.stage[S.wcnt[warp][dg] + rank] = its[r];
+            }
         }
     }
     __syncthreads();
@@ -390,40 +405,37 @@ __global__ void seed_prefix_kernel(const uint32_t *seed_out, uint32_t d, int64_t
 // One pass over the sorted items: in part entry i (key v, value u) goes to
 // col[outprefix(v + 1) + i], and rowptr[x] = outprefix(x) + #items with key < x
 // is written for every x in (key(i-1), key(i)] (i = n_items closes the range up
-// to n; keys >= n -- only after an input error -- count as n).  A thread takes
-// four consecutive items with two 16-byte loads.
+// to n; keys >= n -- only after an input error -- count as n).  Consecutive
+// threads take consecutive items (coalesced stores); a thread's U items of one
+// step are a grid stride apart, their loads issued together.
 template <typename Id>
 __global__ void in_sorted_kernel(const unsigned long long *items, uint64_t n_items, uint64_t n,
                                  uint32_t d, uint64_t seed_edges, const int64_t *seed_pre, Id *col,
                                  uint64_t col_len, int64_t *rowptr)
 {
     constexpr uint32_t U = 4;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x * U;
-    for (uint64_t i0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * U; i0 <= n_items;
-         i0 += stride) {
-        unsigned long long it[U];
-        if (i0 + U <= n_items) {
-            const ulonglong2 a = reinterpret_cast<const ulonglong2 *>(items + i0)[0];
-            const ulonglong2 b = reinterpret_cast<const ulonglong2 *>(items + i0)[1];
-            it[0] = a.x; it[1] = a.y; it[2] = b.x; it[3] = b.y;
-        } else {
-#pragma unroll
-            for (uint32_t q = 0; q < U; ++q) it[q] = i0 + q < n_items ? items[i0 + q] : ~0ull;
-        }
-        uint64_t prev = i0 > 0 ? min((uint64_t)(items[i0 - 1] >> 32), n) : ~0ull;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 <= n_items;
+         i0 += U * stride) {
+        unsigned long long it[U], pv[U];
 #pragma unroll
         for (uint32_t q = 0; q < U; ++q) {
-            const uint64_t i = i0 + q;
+            const uint64_t i = i0 + q * stride;
+            it[q] = i < n_items ? items[i] : ~0ull;
+            pv[q] = i > 0 && i <= n_items ? items[i - 1] : ~0ull;
+        }
+#pragma unroll
+        for (uint32_t q = 0; q < U; ++q) {
+            const uint64_t i = i0 + q * stride;
             if (i > n_items) break;
             const uint64_t v = i < n_items ? min((uint64_t)(it[q] >> 32), n) : n;
-            const uint64_t lo = prev + 1;   // 0 for the first item (prev = ~0)
+            const uint64_t lo = i > 0 ? min((uint64_t)(pv[q] >> 32), n) + 1 : 0;
             for (uint64_t x = lo; x <= v && x <= n; ++x)
                 rowptr[x] = (int64_t)(outprefix(x, d, seed_edges, seed_pre) + i);
             if (i < n_items && v < n) {
                 const uint64_t pos = outprefix(v + 1, d, seed_edges, seed_pre) + i;
                 if (pos < col_len) col[pos] = (Id)(it[q] & 0xffffffffull);
             }
-            prev = v;
         }
     }
 }
@@ -538,8 +550,8 @@ int csr_enqueue_t(const pa_params *prm, const GenPlan &p, const Id *E, int64_t *
         if (rc != PA_OK) return rc;
     }
     const uint64_t col_len = 2 * m;
-    in_sorted_kernel<Id><<<grid_for((m + 4) / 4, 256), 256, 0, s>>>(A, m, n, d, p.seed_edges,
-                                                                    seed_pre, col, col_len, rowptr);
+    in_sorted_kernel<Id><<<grid_for(m / 4 + 1, 256), 256, 0, s>>>(A, m, n, d, p.seed_edges,
+                                                                   seed_pre, col, col_len, rowptr);
     out_part_kernel<Id><<<grid_for(n * d / 4 + 1, 256), 256, 0, s>>>(E, rowptr, col, n, d,
                                                                      p.seed_edges, col_len);
     if (p.wide) {

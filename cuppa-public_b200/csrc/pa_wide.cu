@@ -240,8 +240,8 @@ __global__ void wide_kernel(const GenArgs a, unsigned long long *ticket, uint32_
 uint32_t set_cap_log2(uint32_t d)
 {
     uint32_t lg = 5;
-    while ((1u << lg) < 2u * d && (4u << lg) <= kWideSetMaxBytes) ++lg;
-    while ((1u << lg) <= d) ++lg;
+    while ((1u << lg) < 2u * d && (4u << (lg + 1)) <= kWideSetMaxBytes) ++lg;
+    while ((1u << lg) <= d) ++lg;   // d <= 32767: at most 2^15 slots, 128 KB
     return lg;
 }
 

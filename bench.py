@@ -796,7 +796,8 @@ def measure_served(args, rate: float, seconds: float, outputs_name: str, world: 
     lat, edges_done, statuses = [], 0, []
     outputs = {"pairs": pa.PA_OUT_PAIRS, "csr": pa.PA_OUT_CSR,
                "both": pa.PA_OUT_PAIRS | pa.PA_OUT_CSR}[outputs_name]
-    with pa.Server(budget_bytes=budget, outputs=outputs) as srv, \
+    with pa.Server(budget_bytes=budget, outputs=outputs, max_inflight=args.serve_max_inflight,
+                   express_edges=args.serve_express_edges) as srv, \
             ClockSampler(torch.cuda.current_device()) as clk:
         # warm-up: a few requests, waited for and released
         for q in prms[: args.warmup]:
@@ -928,6 +929,10 @@ def main():
     ap.add_argument("--serve-budget-gb", type=float, default=150.0, help="served: HBM budget")
     ap.add_argument("--serve-outputs", choices=["pairs", "csr", "both"], default="csr",
                     help="served: what each finished request keeps on the device")
+    ap.add_argument("--serve-max-inflight", type=int, default=0,
+                    help="served: batches per lane on the GPU at once (0 = the server's default)")
+    ap.add_argument("--serve-express-edges", type=int, default=0,
+                    help="served: largest request of the express lane (0 = the server's default)")
     ap.add_argument("--no-extras", action="store_true",
                     help="default workload: skip the batched and served figures in its line")
     ap.add_argument("--serve-window", type=float, default=2.0,

@@ -24,6 +24,12 @@
 
 #include "pa_batch.h"
 
+// Resident start-kernel blocks per SM of a batch launch (a start_min_blocks
+// variant: 4, 5 or 6).
+#ifndef PA_BATCH_START_BLOCKS
+#define PA_BATCH_START_BLOCKS gen::kStartMinBlocks
+#endif
+
 namespace pa {
 namespace gen {
 
@@ -359,7 +365,7 @@ int batch_enqueue(const BatchJob &J, void *d_scratch, const void *image, cudaStr
     sa.ticket = tickets;
     sa.ctl = ctl;
     if (J.count == 1) sa.one = J.first;
-    rc = gen::launch_start(J.id_bytes, sa, 0, s);
+    rc = gen::launch_start(J.id_bytes, sa, 0, s, false, PA_BATCH_START_BLOCKS);
     if (rc != PA_OK) return rc;
     return gen::launch_tail(J.id_bytes, J.passes, d_inst, device_tables(J.tail, scr), J.count,
                             J.tail.lvl[0], J.tail.lvl[J.tail.levels], tail_ticket, ctl,

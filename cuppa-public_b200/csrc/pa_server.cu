@@ -1,20 +1,21 @@
 // pa_server.cu -- the request server: continuous batching of generation
 // requests under a device-memory budget.
 //
-// One control thread per server owns the server's CUDA streams and a CUDA
-// memory pool on its device.  Client threads only touch host state (under the
-// server mutex): submit queues a request with the admission queue
-// (pa_sched.cpp), poll/wait read its state, release hands its buffer back.
+// One control thread per server owns the server's CUDA streams and memory
+// pools on its device.  Client threads only touch host state (under the server
+// mutex): submit queues a request with the admission queue (pa_sched.cpp),
+// poll/wait read its state, release hands its buffer back.
 //
 // Two lanes share the budget.  Requests of at most express_edges edges go to
-// the express lane, the rest to the bulk lane; each lane has max_inflight
-// streams of its own (the express lane's at the device's highest stream
-// priority), and a launch goes to the lane's least busy stream.  Kernels are
-// not preempted, but the block scheduler hands SMs that free up to waiting
-// blocks of higher-priority streams first: a small request that arrives while
-// a large batch runs starts at the batch's next kernel boundary (a start
-// kernel's tail, or between its CSR kernels) instead of after the whole batch,
-// and batch k+1 of a lane fills batch k's tail on the lane's other stream.
+// the express lane, the rest to the bulk lane.  Each lane has one stream (the
+// express lane's at the device's highest stream priority), on which up to
+// max_inflight of its launches queue in order, and a memory pool of its own, so
+// that an allocation never waits for memory freed behind the other lane's
+// work.  Kernels are not preempted, but the block scheduler hands SMs that free
+// up to waiting blocks of higher-priority streams first: a small request that
+// arrives while a large batch runs starts at the batch's next kernel boundary
+// (a start kernel's tail, or between its CSR kernels) instead of after the
+// whole batch.
 //
 // The control thread loops, never waiting on the GPU:
 //   1. completions: for each in-flight launch whose event has fired, read the
@@ -23,7 +24,7 @@
 //      of a launch was queued) give their staging buffers back the same way;
 //   2. frees: buffers of released (or TTL-expired) results are freed on the
 //      stream that made them and their budget returned;
-//   3. admission: for each lane with a free stream, admit what fits the budget
+//   3. admission: for each lane with room in flight, admit what fits the budget
 //      and launch it as one batch per id width (the fill / start / tail launches
 //      of pa_batch.cu) -- requests that arrived while earlier batches ran make
 //      up the next; a group whose allocations fail (a fragmented pool) waits,
@@ -106,7 +107,8 @@ struct Job {
 };
 
 struct LaneState {
-    std::vector<cudaStream_t> streams;
+    std::vector<cudaStream_t> streams;             // one stream: launches queue in order
+    cudaMemPool_t pool = nullptr;                  // the lane's own device memory
     std::vector<Launch> inflight;                  // each on one of `streams`
     std::deque<std::pair<std::vector<Job>, bool>> deferred;   // groups (batch?) waiting to
                                                                // be retried after a completion
@@ -150,7 +152,6 @@ struct pa_server {
     // control thread only
     LaneState lanes[kLanes];
     std::vector<Retired> retired;
-    cudaMemPool_t pool = nullptr;
     std::vector<Pinned> pinned_free;
 
     uint64_t now() const
@@ -178,6 +179,8 @@ Pinned get_pinned(pa_server *S, uint64_t bytes)
 }
 
 // Queue a request's buffers for freeing and its budget for return (lock held).
+// Buffers are freed in order on the stream that made them (the lane's stream,
+// whose pool owns them).
 void drop_buffers(pa_server *S, uint64_t tk, Request &r)
 {
     for (void *b : {r.edges, (void *)r.rowptr, r.col})
@@ -227,13 +230,13 @@ void complete(pa_server *S, const std::vector<uint64_t> &tickets, int status, ui
 // fragmented, its memory that is free and no longer in use goes back to the
 // device and the allocation is tried once more; the caller retries later
 // (after a completion) if that fails too.  Nothing here waits for the GPU.
-cudaError_t pool_alloc(pa_server *S, void **p, uint64_t bytes, cudaStream_t s)
+cudaError_t pool_alloc(cudaMemPool_t pool, void **p, uint64_t bytes, cudaStream_t s)
 {
-    cudaError_t e = cudaMallocFromPoolAsync(p, std::max<uint64_t>(bytes, 16), S->pool, s);
+    cudaError_t e = cudaMallocFromPoolAsync(p, std::max<uint64_t>(bytes, 16), pool, s);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
-        cudaMemPoolTrimTo(S->pool, 0);
-        e = cudaMallocFromPoolAsync(p, std::max<uint64_t>(bytes, 16), S->pool, s);
+        cudaMemPoolTrimTo(pool, 0);
+        e = cudaMallocFromPoolAsync(p, std::max<uint64_t>(bytes, 16), pool, s);
         if (e != cudaSuccess) (void)cudaGetLastError();
     }
     return e;
@@ -282,9 +285,9 @@ bool launch_group(pa_server *S, const std::vector<Job> &jobs, bool batch, uint32
     int rc = PA_OK;
     cudaError_t e = cudaSuccess;
     for (uint32_t i = 0; i < k && e == cudaSuccess; ++i) {
-        e = pool_alloc(S, &edges[i], ebytes[i], st);
-        if (csr && e == cudaSuccess) e = pool_alloc(S, &rowptr[i], jobs[i].rowptr_bytes, st);
-        if (csr && e == cudaSuccess) e = pool_alloc(S, &col[i], jobs[i].col_bytes, st);
+        e = pool_alloc(LS.pool, &edges[i], ebytes[i], st);
+        if (csr && e == cudaSuccess) e = pool_alloc(LS.pool, &rowptr[i], jobs[i].rowptr_bytes, st);
+        if (csr && e == cudaSuccess) e = pool_alloc(LS.pool, &col[i], jobs[i].col_bytes, st);
     }
     BatchJob J;
     uint64_t scratch_bytes = 0, image_bytes = 0;
@@ -296,7 +299,7 @@ bool launch_group(pa_server *S, const std::vector<Job> &jobs, bool batch, uint32
         } else {
             rc = pa_scratch_bytes(&prms[0], &scratch_bytes);
         }
-        if (rc == PA_OK) e = pool_alloc(S, &L.scratch, scratch_bytes, st);
+        if (rc == PA_OK) e = pool_alloc(LS.pool, &L.scratch, scratch_bytes, st);
     }
     if (e != cudaSuccess && may_defer) {
         // nothing queued yet: give the memory back (stream-ordered) and wait
@@ -336,7 +339,7 @@ bool launch_group(pa_server *S, const std::vector<Job> &jobs, bool batch, uint32
             csr_status[i] = PA_OK;
             continue;
         }
-        e = pool_alloc(S, &cscr[i], jobs[i].csr_scratch, st);
+        e = pool_alloc(LS.pool, &cscr[i], jobs[i].csr_scratch, st);
         if (e != cudaSuccess) {
             rc = set_cuda_error(e);
             break;
@@ -443,7 +446,7 @@ void control_loop(pa_server *S)
 {
     cudaSetDevice(S->device);
     const uint32_t max_batch = S->cfg.max_batch ? S->cfg.max_batch : 4096u;
-    const uint32_t max_inflight = S->cfg.max_inflight ? S->cfg.max_inflight : 2u;
+    const uint32_t max_inflight = S->cfg.max_inflight ? S->cfg.max_inflight : 4u;
     std::vector<uint64_t> adm(max_batch);
     for (;;) {
         bool progressed = false, freed = false;
@@ -605,7 +608,6 @@ int pa_server_create(const pa_server_config *cfg, pa_server **out)
     if (!S) return PA_ERR_OOM;
     S->cfg = *cfg;
     S->express_edges = cfg->express_edges ? cfg->express_edges : kExpressEdgesAuto;
-    const uint32_t max_inflight = cfg->max_inflight ? cfg->max_inflight : 2u;
     int prev = 0;
     cudaError_t e = cudaGetDevice(&prev);
     S->device = cfg->device >= 0 ? cfg->device : prev;
@@ -614,33 +616,34 @@ int pa_server_create(const pa_server_config *cfg, pa_server **out)
     if (e == cudaSuccess) e = cudaMemGetInfo(&free_b, &total_b);
     int least = 0, greatest = 0;
     if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
-    for (uint32_t lane = 0; lane < kLanes && e == cudaSuccess; ++lane)
-        for (uint32_t i = 0; i < max_inflight && e == cudaSuccess; ++i) {
-            cudaStream_t s = nullptr;
-            e = cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking,
-                                             lane == kExpress ? greatest : least);
-            if (e == cudaSuccess) S->lanes[lane].streams.push_back(s);
+    for (uint32_t lane = 0; lane < kLanes && e == cudaSuccess; ++lane) {
+        LaneState &LS = S->lanes[lane];
+        cudaStream_t s = nullptr;
+        e = cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking,
+                                         lane == kExpress ? greatest : least);
+        if (e == cudaSuccess) LS.streams.push_back(s);
+        if (e == cudaSuccess) {
+            cudaMemPoolProps props;
+            std::memset(&props, 0, sizeof(props));
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = S->device;
+            e = cudaMemPoolCreate(&LS.pool, &props);
         }
-    if (e == cudaSuccess) {
-        cudaMemPoolProps props;
-        std::memset(&props, 0, sizeof(props));
-        props.allocType = cudaMemAllocationTypePinned;
-        props.location.type = cudaMemLocationTypeDevice;
-        props.location.id = S->device;
-        e = cudaMemPoolCreate(&S->pool, &props);
+        if (e == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;   // freed blocks stay with the pool for reuse
+            e = cudaMemPoolSetAttribute(LS.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
     }
-    if (e == cudaSuccess) {
-        uint64_t keep = UINT64_MAX;   // freed blocks stay with the pool for reuse
-        e = cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    }
-    auto destroy_streams = [&] {
-        for (LaneState &LS : S->lanes)
+    auto destroy_lanes = [&] {
+        for (LaneState &LS : S->lanes) {
             for (cudaStream_t s : LS.streams) cudaStreamDestroy(s);
+            if (LS.pool) cudaMemPoolDestroy(LS.pool);
+        }
     };
     cudaSetDevice(prev);
     if (e != cudaSuccess) {
-        if (S->pool) cudaMemPoolDestroy(S->pool);
-        destroy_streams();
+        destroy_lanes();
         delete S;
         return set_cuda_error(e);
     }
@@ -649,8 +652,7 @@ int pa_server_create(const pa_server_config *cfg, pa_server **out)
     if (S->cfg.outputs == 0) S->cfg.outputs = PA_OUT_PAIRS;
     S->sched = pa_sched_create(S->cfg.budget_bytes, S->cfg.aging_ns, S->cfg.max_queue);
     if (!S->sched) {
-        cudaMemPoolDestroy(S->pool);
-        destroy_streams();
+        destroy_lanes();
         delete S;
         return PA_ERR_OOM;
     }
@@ -786,9 +788,10 @@ int pa_server_destroy(pa_server *S)
     }
     if (S->worker.joinable()) S->worker.join();
     for (auto &b : S->pinned_free) cudaFreeHost(b.p);
-    cudaMemPoolDestroy(S->pool);
-    for (LaneState &LS : S->lanes)
+    for (LaneState &LS : S->lanes) {
         for (cudaStream_t s : LS.streams) cudaStreamDestroy(s);
+        cudaMemPoolDestroy(LS.pool);
+    }
     pa_sched_destroy(S->sched);
     delete S;
     return PA_OK;

@@ -255,10 +255,10 @@ int pa_batch_generate(const pa_params *prms, uint32_t count, void *const *d_edge
  * batches on the GPU -- so requests that arrive while a batch runs form the
  * next one -- and marks each request done when its batch's completion event
  * has fired; it never waits on the GPU.  Two lanes share the budget: requests
- * of at most express_edges edges run in the express lane, on streams of the
- * device's highest priority, so a small request that arrives while a large
- * batch runs starts at that batch's next kernel boundary; each lane has
- * max_inflight streams, so a lane's next batch fills the previous one's tail.
+ * of at most express_edges edges run in the express lane, on a stream of the
+ * device's highest priority with a memory pool of its own, so a small request
+ * that arrives while a large batch runs starts at that batch's next kernel
+ * boundary; a lane's launches queue in order on its stream.
  * A result stays in device memory, owned by the server, until
  * pa_server_release (or until it has been finished for ttl_ns).  Submit, poll,
  * wait and release may be called from any thread. */
@@ -272,8 +272,7 @@ enum { PA_OUT_PAIRS = 1, PA_OUT_CSR = 2 };
 typedef struct pa_server_config {
     uint64_t budget_bytes;   /* device memory for admitted requests; 0 = 3/4 of free memory */
     uint32_t max_batch;      /* requests per launch; 0 = 4096                              */
-    uint32_t max_inflight;   /* batches on the GPU at once per lane (each on its own
-                                stream); 0 = 2                                             */
+    uint32_t max_inflight;   /* batches queued on the GPU at once per lane; 0 = 4          */
     uint32_t max_queue;      /* queued (not yet admitted) requests; 0 = unlimited          */
     int32_t device;          /* CUDA device; -1 = the caller's current device              */
     uint64_t ttl_ns;         /* finished results unreleased this long are freed; 0 = never */

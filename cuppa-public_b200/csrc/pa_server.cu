@@ -656,6 +656,25 @@ int pa_server_create(const pa_server_config *cfg, pa_server **out)
         delete S;
         return PA_ERR_OOM;
     }
+    // Map each lane's share of the budget into its pool now (allocated once and
+    // freed; the pool keeps freed memory), so that serving does not grow the
+    // pools -- a driver mapping on the control thread -- while requests wait.
+    // The express lane's requests are small: an eighth of the budget.
+    if (S->cfg.budget_bytes) {
+        cudaSetDevice(S->device);
+        for (uint32_t lane = 0; lane < kLanes; ++lane) {
+            LaneState &LS = S->lanes[lane];
+            const uint64_t share = lane == kExpress ? S->cfg.budget_bytes / 8
+                                                    : S->cfg.budget_bytes - S->cfg.budget_bytes / 8;
+            void *p = nullptr;
+            if (cudaMallocFromPoolAsync(&p, share, LS.pool, LS.streams[0]) == cudaSuccess)
+                cudaFreeAsync(p, LS.streams[0]);
+            else
+                (void)cudaGetLastError();   // best effort: the pool grows on demand instead
+            cudaStreamSynchronize(LS.streams[0]);
+        }
+        cudaSetDevice(prev);
+    }
     S->st.budget_bytes = S->cfg.budget_bytes;
     S->t0 = std::chrono::steady_clock::now();
     S->worker = std::thread(control_loop, S);

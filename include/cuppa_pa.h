@@ -72,7 +72,8 @@ enum { PA_LAYOUT_PAIRS = 0, PA_LAYOUT_SLOTS = 1 };
 
 typedef struct pa_params {
     uint64_t n;             /* nodes                        (-n/--n1; cuPPA(n, ...))      */
-    uint32_t d;             /* edges per new node, 1..32    (-x/--x1; M)                  */
+    uint32_t d;             /* edges per new node, 1..32767 (-x/--x1; M; the reference's int16
+                               EdgeIndexType, src/Common/DataTypes.h:11-28)               */
     uint32_t id_bits;       /* 32 or 64: width of each stored id                           */
     double p;               /* probability of a direct pick (-a/--alpha), 0 <= p <= 1      */
     uint64_t seed;          /* Philox key                                                 */

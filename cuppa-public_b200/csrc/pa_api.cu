@@ -142,7 +142,8 @@ int pa_params_check(const pa_params *prm)
         prm->tile_passes != 4 && prm->tile_passes != 8)
         return PA_ERR_INVALID;
     if (prm->threads != 0 && prm->threads != 256) return PA_ERR_NOT_SUPPORTED;
-    if ((prm->flags & ~PA_FLAG_TEST_WITHHOLD_FIRST_TILE) != 0) return PA_ERR_INVALID;
+    if ((prm->flags & ~(PA_FLAG_TEST_WITHHOLD_FIRST_TILE | PA_FLAG_PREFILLED)) != 0)
+        return PA_ERR_INVALID;
     if (prm->claim_tiles > 64) return PA_ERR_INVALID;
     if (prm->model != PA_MODEL_COPY && prm->model != PA_MODEL_BA) return PA_ERR_INVALID;
     if (prm->model == PA_MODEL_BA && prm->seed_mode != PA_SEED_STAR_REF) return PA_ERR_INVALID;
@@ -201,6 +202,16 @@ int pa_generate(const pa_params *prm, void *d_edges, uint64_t edges_bytes, void 
         return PA_ERR_INVALID;
     if (edges_bytes < p.edges_bytes || scratch_bytes < p.scratch_bytes) return PA_ERR_CAPACITY;
     return launch_generate(prm, p, d_edges, d_scratch, (cudaStream_t)stream, 0);
+}
+
+int pa_fill(const pa_params *prm, void *d_edges, uint64_t edges_bytes, void *stream)
+{
+    GenPlan p;
+    const int rc = make_plan(prm, &p);
+    if (rc != PA_OK) return rc;
+    if (!d_edges || (reinterpret_cast<uintptr_t>(d_edges) & 15u)) return PA_ERR_INVALID;
+    if (edges_bytes < p.edges_bytes) return PA_ERR_CAPACITY;
+    return fill_prefill(prm, p, d_edges, (cudaStream_t)stream);
 }
 
 int pa_generate_timed(const pa_params *prm, void *d_edges, uint64_t edges_bytes, void *d_scratch,

@@ -358,6 +358,65 @@ int launch_passes(const GenArgs &a, uint32_t passes, uint32_t blocks, cudaStream
 
 }  // namespace
 
+// Bytes [*off, *off + *len) of the edge buffer that a generation fills with
+// all-ones before its kernels run: the slots of the start kernel's nodes (every
+// node, for d > 32), after the seed edges.
+void fill_region(const pa_params &prm, const GenPlan &plan, uint64_t *off, uint64_t *len)
+{
+    const uint64_t slot_bytes = (plan.slots ? 1ull : 2ull) * plan.id_bytes;
+    const uint64_t seed = plan.slots ? 0 : plan.seed_edges;
+    const uint64_t end = plan.wide ? prm.n : plan.u_split;
+    *off = seed * slot_bytes;
+    *len = end > plan.u_first ? (end - plan.u_first) * prm.d * slot_bytes : 0;
+}
+
+namespace {
+
+// All-ones over bytes [lo, hi) of p: 16-byte stores over the aligned body, the
+// ragged ends byte by byte from the first thread.  One small block per SM, so
+// that a generation on another stream keeps its own blocks resident beside it.
+__global__ void __launch_bounds__(128) fill_ones_kernel(unsigned char *p, uint64_t lo, uint64_t hi)
+{
+    const uint64_t a = (lo + 15) & ~15ull, b = hi & ~15ull;
+    if (a >= b) {
+        if (blockIdx.x == 0 && threadIdx.x == 0)
+            for (uint64_t i = lo; i < hi; ++i) p[i] = 0xff;
+        return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (uint64_t i = lo; i < a; ++i) p[i] = 0xff;
+        for (uint64_t i = b; i < hi; ++i) p[i] = 0xff;
+    }
+    uint4 *q = reinterpret_cast<uint4 *>(p + a);
+    const uint64_t n16 = (b - a) >> 4;
+    const uint4 ones = make_uint4(~0u, ~0u, ~0u, ~0u);
+    // eight stores per thread per step keep enough writes in flight for a grid
+    // this small
+    constexpr uint32_t U = 8;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; x + (U - 1) * stride < n16; x += U * stride) {
+#pragma unroll
+        for (uint32_t j = 0; j < U; ++j) q[x + j * stride] = ones;
+    }
+    for (; x < n16; x += stride) q[x] = ones;
+}
+
+}  // namespace
+
+int fill_prefill(const pa_params *prm, const GenPlan &plan, void *d_edges, cudaStream_t s)
+{
+    uint64_t off = 0, len = 0;
+    fill_region(*prm, plan, &off, &len);
+    if (len == 0) return PA_OK;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    fill_ones_kernel<<<sms, 128, 0, s>>>(reinterpret_cast<unsigned char *>(d_edges), off, off + len);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PA_OK : set_cuda_error(e);
+}
+
 int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, void *d_scratch,
                     cudaStream_t stream, uint32_t blocks_override, const cudaEvent_t *events)
 {
@@ -412,12 +471,15 @@ int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, vo
 
 
     const uint32_t blocks = blocks_override ? blocks_override : prm->blocks;
+    const bool prefilled = (prm->flags & PA_FLAG_PREFILLED) != 0;
     if (plan.wide) {
         // every node by the wide kernel, its slots starting as all-ones
-        const uint64_t slot_bytes = (plan.slots ? 1ull : 2ull) * plan.id_bytes;
-        e = cudaMemsetAsync(reinterpret_cast<unsigned char *>(d_edges) + a.seed_edges * slot_bytes,
-                            0xff, (prm->n - plan.u_first) * prm->d * slot_bytes, stream);
-        if (e != cudaSuccess) return set_cuda_error(e);
+        uint64_t off = 0, len = 0;
+        fill_region(*prm, plan, &off, &len);
+        if (!prefilled) {
+            e = cudaMemsetAsync(reinterpret_cast<unsigned char *>(d_edges) + off, 0xff, len, stream);
+            if (e != cudaSuccess) return set_cuda_error(e);
+        }
         a.start_end = prm->n;
         if ((mrc = mark(1)) != PA_OK) return mrc;
         const int rc = launch_wide(plan.id_bytes, plan.slots, a,
@@ -435,10 +497,12 @@ int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, vo
         // The start region, with slot-granular waits (pa_start.cu): its pairs
         // (ids, in SLOTS) start as all-ones; the start kernel writes them and
         // the seed edges.
-        const uint64_t slot_bytes = (plan.slots ? 1ull : 2ull) * plan.id_bytes;
-        e = cudaMemsetAsync(reinterpret_cast<unsigned char *>(d_edges) + a.seed_edges * slot_bytes,
-                            0xff, (plan.u_split - plan.u_first) * prm->d * slot_bytes, stream);
-        if (e != cudaSuccess) return set_cuda_error(e);
+        if (!prefilled) {
+            uint64_t off = 0, len = 0;
+            fill_region(*prm, plan, &off, &len);
+            e = cudaMemsetAsync(reinterpret_cast<unsigned char *>(d_edges) + off, 0xff, len, stream);
+            if (e != cudaSuccess) return set_cuda_error(e);
+        }
         StartArgs sa;
         std::memset(&sa, 0, sizeof(sa));
         sa.one = a;

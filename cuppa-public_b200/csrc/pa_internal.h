@@ -94,6 +94,11 @@ constexpr uint64_t kStartNodesAuto = 1ull << 31;
 int csr_enqueue(const pa_params *prm, const void *d_edges, int64_t *d_rowptr, void *d_col,
                 void *d_scratch, uint64_t scratch_bytes, cudaStream_t s, uint64_t *err_offset);
 
+// The all-ones region of a generation (byte offset and length in the edge
+// buffer), and a fill of it on a small grid (pa_fill).
+void fill_region(const pa_params &prm, const GenPlan &plan, uint64_t *off, uint64_t *len);
+int fill_prefill(const pa_params *prm, const GenPlan &plan, void *d_edges, cudaStream_t s);
+
 int launch_generate(const pa_params *prm, const GenPlan &plan, void *d_edges, void *d_scratch,
                     cudaStream_t stream, uint32_t blocks_override,
                     const cudaEvent_t *events = nullptr);

@@ -53,6 +53,8 @@ PA_FORMAT_BINARY = 1
 # Test-only: the generator never publishes its first tile, so every wait on it
 # runs into the wait limit (a flag that nothing sets).
 PA_FLAG_TEST_WITHHOLD_FIRST_TILE = 1 << 31
+# the edge buffer's generation region was set to all-ones by fill(): skip the fill
+PA_FLAG_PREFILLED = 1
 # start_nodes: no start kernel (every node in the persistent launch)
 PA_START_NONE = (1 << 64) - 1
 # request server outputs (a mask)
@@ -167,6 +169,7 @@ _SIGS = {
     "pa_generate": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_uint64,
                                    ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),
     "pa_generate_finish": (ctypes.c_int, [ctypes.c_void_p, _P(PaStats), ctypes.c_void_p]),
+    "pa_fill": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]),
     "pa_start_split": (ctypes.c_int, [_P(PaParams), _P(ctypes.c_uint64)]),
     "pa_generate_timed": (ctypes.c_int, [_P(PaParams), ctypes.c_void_p, ctypes.c_uint64,
                                          ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
@@ -334,6 +337,15 @@ def generate_into(prm: PaParams, edges, scratch, stream=None) -> None:
                            ctypes.c_void_p(scratch.data_ptr()), scratch.numel(),
                            ctypes.c_void_p(_stream_ptr(stream)))
     check(rc, "pa_generate")
+
+
+def fill(prm: PaParams, edges, stream=None) -> None:
+    """pa_fill: all-ones over the generation region of `edges`, on a small grid
+    that can run beside a generation on another stream (for a later generation
+    with PA_FLAG_PREFILLED)."""
+    check(lib().pa_fill(ctypes.byref(prm), ctypes.c_void_p(edges.data_ptr()),
+                        edges.numel() * edges.element_size(),
+                        ctypes.c_void_p(_stream_ptr(stream))), "pa_fill")
 
 
 def generate_timed(prm: PaParams, edges, scratch, events, stream=None) -> None:

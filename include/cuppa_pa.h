@@ -67,6 +67,10 @@ enum { PA_LAYOUT_PAIRS = 0, PA_LAYOUT_SLOTS = 1 };
  * the generator never publishes its first tile, so every wait on that tile runs
  * into spin_limit_ns and the call reports PA_ERR_SPIN_TIMEOUT. */
 #define PA_FLAG_TEST_WITHHOLD_FIRST_TILE 0x80000000u
+/* PREFILLED: the caller has already set d_edges' generation region to
+ * all-ones with pa_fill (on any stream, ordered before the generation), so the
+ * generation skips its own fill. */
+#define PA_FLAG_PREFILLED 0x1u
 /* (with a start kernel, its first warp pass is withheld instead: the first
  *  nodes' slots are never written, with the same outcome) */
 
@@ -152,6 +156,15 @@ int pa_generate(const pa_params *prm, void *d_edges, uint64_t edges_bytes, void 
  * 217-223). */
 int pa_generate_timed(const pa_params *prm, void *d_edges, uint64_t edges_bytes, void *d_scratch,
                       uint64_t scratch_bytes, void *stream, void *const *events);
+/* Set the generation region of d_edges -- every slot a generation writes and
+ * reads back, the seed edges aside -- to all-ones, the "not yet written" mark
+ * the generators wait on, for a later generation with PA_FLAG_PREFILLED.  The
+ * fill runs on a small grid (one 128-thread block per SM), so it can run beside
+ * a generation on another stream: a caller that generates graphs back to back
+ * into two buffers fills the next buffer while the current one is generated.
+ * Queued on `stream`.  No counterpart in the reference, whose per-batch fill
+ * (src/PA/cuPPA/cuPPA_RRP.cu:78-102) sits inside its stage loop. */
+int pa_fill(const pa_params *prm, void *d_edges, uint64_t edges_bytes, void *stream);
 /* Wait for the stream, then copy the status and counters of the generation that
  * last used d_scratch.  Returns the device status. */
 int pa_generate_finish(const void *d_scratch, pa_stats *out, void *stream);

@@ -80,7 +80,7 @@ def test_param_checks(pa):
     assert rc(id_bits=64, n=2 ** 31) == pa.PA_OK
     assert rc(seed_mode=7) == pa.PA_ERR_INVALID
     assert rc(tile_passes=3) == pa.PA_ERR_INVALID
-    assert rc(flags=1) == pa.PA_ERR_INVALID
+    assert rc(flags=2) == pa.PA_ERR_INVALID
     assert rc(flags=pa.PA_FLAG_TEST_WITHHOLD_FIRST_TILE) == pa.PA_OK
 
 
@@ -185,3 +185,13 @@ def test_digest_rejects_bad_arguments_without_touching_the_device(pa):
     assert L.pa_digest(ctypes.c_void_p(4096), 10, 64, 0, ctypes.c_void_p(4100), None) == \
         pa.PA_ERR_INVALID
     assert L.pa_digest(None, 0, 32, 0, acc, None) == pa.PA_OK     # nothing to do
+
+
+def test_fill_checks_and_prefilled_flag(pa):
+    L = pa.lib()
+    prm = pa.make_params(1000, 4, 0.5)
+    assert L.pa_fill(ctypes.byref(prm), None, 1 << 20, None) == pa.PA_ERR_INVALID
+    assert L.pa_fill(ctypes.byref(prm), ctypes.c_void_p(4104), 1 << 20, None) == pa.PA_ERR_INVALID
+    assert L.pa_fill(ctypes.byref(prm), ctypes.c_void_p(4096), 16, None) == pa.PA_ERR_CAPACITY
+    prm.flags = pa.PA_FLAG_PREFILLED
+    assert L.pa_params_check(ctypes.byref(prm)) == pa.PA_OK

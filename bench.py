@@ -742,7 +742,7 @@ def measure_batched(args, world: int, rank: int):
         waves.append(cur)
 
     stream = torch.cuda.Stream()
-    t_batch = t_plain = 0.0
+    t_batch = t_plain = dev_batch = 0.0
     digests_b, digests_p = {}, {}
     total_edges = 0
     with ClockSampler(torch.cuda.current_device()) as clk:
@@ -755,10 +755,14 @@ def measure_batched(args, world: int, rank: int):
                 batch.generate(stream)
                 pa.check(batch.finish(stream).status, "batched warm-up")
             torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             t0 = time.perf_counter()
+            e0.record(stream)
             batch.generate(stream)
+            e1.record(stream)
             st = batch.finish(stream)   # waits
             t_batch += time.perf_counter() - t0
+            dev_batch += e0.elapsed_time(e1) / 1e3
             pa.check(st.status, "batched generation")
             for k, i in enumerate(wave):
                 digests_b[i] = pa.digest(batch.graph(k).reshape(-1), stream=stream)
@@ -790,6 +794,7 @@ def measure_batched(args, world: int, rank: int):
         "graphs_per_s": n_graphs / t_batch, "ms": t_batch * 1e3,
         "plain_graphs_per_s": n_graphs / t_plain, "plain_ms": t_plain * 1e3,
         "speedup_vs_plain": t_plain / t_batch, "identical_outputs": same,
+        "device_ms": dev_batch * 1e3,
         "edges": total_edges, "edges_per_s": total_edges / t_batch,
         "waves_rank0": len(waves), "wave_budget_gb": args.budget_gb,
         "timing": "host clock around each wave's launches and its completion wait",

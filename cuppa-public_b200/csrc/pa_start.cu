@@ -109,22 +109,33 @@ __device__ __forceinline__ bool resolve_start(Slot<uint32_t> (&s)[kStartPasses],
     const uint32_t max_sleep = min(a.max_sleep_ns, 512u);
     uint64_t spin_t0 = 0;
     uint32_t sleep_ns = 32;
+    // bit j: every active slot of pass j is final and stored (warp-uniform); a
+    // finished pass costs no more match or ballot while the others wait
+    uint32_t done = 0;
+    // bit j: this lane's slot of pass j changed after the pass's last match; a
+    // pass in which no lane changed would match and vote exactly as before, so
+    // only its pending reads are polled (one vote per pass and round)
+    uint32_t dirty = (1u << kStartPasses) - 1u;
     for (;;) {
         bool changed = false;
-        bool all_fin = true;
 #pragma unroll
         for (int j = 0; j < kStartPasses; ++j) {
+            if ((done >> j) & 1u) continue;
             const uint32_t pbase = tb + j * G;
             const uint32_t u = pbase + L.g;
             const bool active = L.used && u < a.start_end;
+            bool ch = (dirty >> j) & 1u;
             if (active && meta_st(s[j].meta) == ST_PEND_GLOBAL) {
                 if (read_slot<Id, Slots>(s[j], a, E, s[j].val, meta_k(s[j].meta))) {
                     s[j].meta &= ~3u;
+                    ch = true;
                     changed = true;
                 } else {
                     ++n_poll;
                 }
             }
+            if (!__any_sync(kFull, ch)) continue;
+            dirty &= ~(1u << j);
             const bool known = active && meta_st(s[j].meta) == ST_KNOWN;
             // node values are < 2^31: the lane-unique keys of unknown lanes never collide
             const uint32_t eq = __match_any_sync(kFull, known ? s[j].val : (0xffffffe0u | L.lane));
@@ -139,8 +150,10 @@ __device__ __forceinline__ bool resolve_start(Slot<uint32_t> (&s)[kStartPasses],
                 stored |= 1u << j;
             }
             const uint32_t finm = __ballot_sync(kFull, fin || !active);
-            if (finm == kFull) continue;
-            all_fin = false;
+            if (finm == kFull) {
+                done |= 1u << j;
+                continue;
+            }
 
             // copy sources in this pass: the source lane's value once it is final
             const bool same = active && meta_st(s[j].meta) == ST_PEND_TILE;
@@ -149,6 +162,7 @@ __device__ __forceinline__ bool resolve_start(Slot<uint32_t> (&s)[kStartPasses],
             if (same && ((finm >> src) & 1u)) {
                 s[j].val = sv;
                 s[j].meta &= ~3u;
+                dirty |= 1u << j;
                 changed = true;
             }
 
@@ -157,11 +171,12 @@ __device__ __forceinline__ bool resolve_start(Slot<uint32_t> (&s)[kStartPasses],
                 const uint32_t r = meta_r(s[j].meta) + 1u;
                 classify_start<Id, Slots>(s[j], draw<uint32_t>(u, L.slot, r, a), r, a, E, pbase,
                                           n_pend);
+                dirty |= 1u << j;
                 changed = true;
                 ++n_retry;
             }
         }
-        if (all_fin) return true;
+        if (done == (1u << kStartPasses) - 1u) return true;
 
         if (!__any_sync(kFull, changed)) {
             unsigned long long now = 0;

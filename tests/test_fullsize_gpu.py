@@ -142,6 +142,17 @@ def test_c3_full_size(pa, cuda_ok, p):
     free()
 
 
+def test_c3_full_size_int32(pa, cuda_ok):
+    """The same graph with 32-bit ids (34 GB): the digest takes ids sign-extended,
+    so the 64-bit configuration's fixture applies."""
+    prm = pa.make_params(2 ** 30, 4, 0.5, seed=1234, id_bits=32, seed_mode=pa.PA_SEED_CLIQUE)
+    E, st = pa.generate(prm)
+    assert st.status == 0
+    assert pa.digest(E.reshape(-1)) == fixture("c3_p0.5")["pairs"]
+    del E
+    free()
+
+
 def test_sba_full_size(pa, cuda_ok):
     """The BA model (-A sba) at n = 2^30, d = 4, int64, star seed, Philox seed 1234."""
     n, d, seed = 2 ** 30, 4, 1234

@@ -18,7 +18,6 @@
 #include <unordered_map>
 
 #include "cuppa_pa.h"
-#include "pa_sched.h"
 
 struct pa_sched {
     struct Item {
@@ -32,9 +31,10 @@ struct pa_sched {
     mutable std::mutex mu;
 };
 
-namespace pa {
+extern "C" {
 
-int sched_submit_lane(pa_sched *q, uint64_t ticket, uint64_t bytes, uint64_t now_ns, uint32_t lane)
+int pa_sched_submit_lane(pa_sched *q, uint64_t ticket, uint64_t bytes, uint64_t now_ns,
+                         uint32_t lane)
 {
     if (!q || lane >= 32) return PA_ERR_INVALID;
     std::lock_guard<std::mutex> lk(q->mu);
@@ -47,8 +47,8 @@ int sched_submit_lane(pa_sched *q, uint64_t ticket, uint64_t bytes, uint64_t now
     return PA_OK;
 }
 
-uint32_t sched_admit_lanes(pa_sched *q, uint64_t now_ns, uint64_t *out, uint32_t cap,
-                           uint32_t lane_mask)
+uint32_t pa_sched_admit_lanes(pa_sched *q, uint64_t now_ns, uint64_t *out, uint32_t cap,
+                              uint32_t lane_mask)
 {
     if (!q || !out || cap == 0) return 0;
     std::lock_guard<std::mutex> lk(q->mu);
@@ -73,10 +73,6 @@ uint32_t sched_admit_lanes(pa_sched *q, uint64_t now_ns, uint64_t *out, uint32_t
     return n;
 }
 
-}  // namespace pa
-
-extern "C" {
-
 pa_sched *pa_sched_create(uint64_t budget_bytes, uint64_t aging_ns, uint32_t max_queue)
 {
     pa_sched *q = new (std::nothrow) pa_sched();
@@ -91,12 +87,12 @@ void pa_sched_destroy(pa_sched *q) { delete q; }
 
 int pa_sched_submit(pa_sched *q, uint64_t ticket, uint64_t bytes, uint64_t now_ns)
 {
-    return pa::sched_submit_lane(q, ticket, bytes, now_ns, 0);
+    return pa_sched_submit_lane(q, ticket, bytes, now_ns, 0);
 }
 
 uint32_t pa_sched_admit(pa_sched *q, uint64_t now_ns, uint64_t *out, uint32_t cap)
 {
-    return pa::sched_admit_lanes(q, now_ns, out, cap, ~0u);
+    return pa_sched_admit_lanes(q, now_ns, out, cap, ~0u);
 }
 
 int pa_sched_release(pa_sched *q, uint64_t ticket, uint64_t bytes)

@@ -50,7 +50,6 @@
 #include <vector>
 
 #include "pa_batch.h"
-#include "pa_sched.h"
 
 namespace pa {
 namespace {
@@ -552,7 +551,7 @@ void control_loop(pa_server *S)
             {
                 std::lock_guard<std::mutex> lk(S->mu);
                 const uint64_t t = S->now();
-                const uint32_t n = sched_admit_lanes(S->sched, t, adm.data(), max_batch, 1u << lane);
+                const uint32_t n = pa_sched_admit_lanes(S->sched, t, adm.data(), max_batch, 1u << lane);
                 groups = make_groups(S, adm.data(), n, t);
             }
             for (auto &g : groups) {
@@ -705,10 +704,10 @@ int pa_server_submit(pa_server *S, const pa_params *prm, uint64_t *ticket)
     if (S->stop) return PA_ERR_INVALID;
     r.t_submit = S->now();
     const uint64_t tk = S->next_ticket++;
-    rc = sched_submit_lane(S->sched, tk,
-                           r.edges_bytes + r.scratch_reserve + r.rowptr_bytes + r.col_bytes +
-                               r.csr_scratch,
-                           r.t_submit, r.lane);
+    rc = pa_sched_submit_lane(S->sched, tk,
+                              r.edges_bytes + r.scratch_reserve + r.rowptr_bytes + r.col_bytes +
+                                  r.csr_scratch,
+                              r.t_submit, r.lane);
     if (rc != PA_OK) return rc;
     S->reqs.emplace(tk, r);
     ++S->st.submitted;

@@ -239,6 +239,11 @@ _SIGS = {
                                        ctypes.c_uint64]),
     "pa_sched_admit": (ctypes.c_uint32, [ctypes.c_void_p, ctypes.c_uint64, _P(ctypes.c_uint64),
                                          ctypes.c_uint32]),
+    "pa_sched_submit_lane": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                            ctypes.c_uint64, ctypes.c_uint32]),
+    "pa_sched_admit_lanes": (ctypes.c_uint32, [ctypes.c_void_p, ctypes.c_uint64,
+                                               _P(ctypes.c_uint64), ctypes.c_uint32,
+                                               ctypes.c_uint32]),
     "pa_sched_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64]),
     "pa_sched_in_use": (ctypes.c_uint64, [ctypes.c_void_p]),
     "pa_sched_queued": (ctypes.c_uint64, [ctypes.c_void_p]),
@@ -729,12 +734,17 @@ class Sched:
 
     __del__ = close
 
-    def submit(self, ticket: int, nbytes: int, now_ns: int) -> int:
-        return lib().pa_sched_submit(self._h, ticket, nbytes, now_ns)
+    def submit(self, ticket: int, nbytes: int, now_ns: int, lane: int = 0) -> int:
+        if lane == 0:
+            return lib().pa_sched_submit(self._h, ticket, nbytes, now_ns)
+        return lib().pa_sched_submit_lane(self._h, ticket, nbytes, now_ns, lane)
 
-    def admit(self, now_ns: int, cap: int = 4096) -> list:
+    def admit(self, now_ns: int, cap: int = 4096, lanes: int = 0xFFFFFFFF) -> list:
         out = (ctypes.c_uint64 * cap)()
-        n = lib().pa_sched_admit(self._h, now_ns, out, cap)
+        if lanes == 0xFFFFFFFF:
+            n = lib().pa_sched_admit(self._h, now_ns, out, cap)
+        else:
+            n = lib().pa_sched_admit_lanes(self._h, now_ns, out, cap, lanes)
         return [int(out[i]) for i in range(n)]
 
     def release(self, ticket: int, nbytes: int = (1 << 64) - 1) -> int:

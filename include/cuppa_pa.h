@@ -361,6 +361,14 @@ uint32_t pa_sched_admit(pa_sched *q, uint64_t now_ns, uint64_t *out, uint32_t ca
  * is UINT64_MAX, which also forgets the ticket; a queued request is withdrawn).
  * PA_ERR_NOT_FOUND if unknown. */
 int pa_sched_release(pa_sched *q, uint64_t ticket, uint64_t bytes);
+/* Lanes (the request server keeps small requests in a lane of their own): a
+ * request queued in `lane` (0..31) is admitted only by scans that include its
+ * lane in lane_mask; an aged request that does not fit stops the admission of
+ * its own lane only.  pa_sched_submit / pa_sched_admit are lane 0 and all lanes. */
+int pa_sched_submit_lane(pa_sched *q, uint64_t ticket, uint64_t bytes, uint64_t now_ns,
+                         uint32_t lane);
+uint32_t pa_sched_admit_lanes(pa_sched *q, uint64_t now_ns, uint64_t *out, uint32_t cap,
+                              uint32_t lane_mask);
 uint64_t pa_sched_in_use(const pa_sched *q);
 uint64_t pa_sched_queued(const pa_sched *q);
 

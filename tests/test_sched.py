@@ -116,3 +116,83 @@ def test_matches_policy_model(pa, seed):
             got.append(q.release(op[1]))
     assert got == want
     assert q.in_use == used
+
+
+def test_lanes_admit_separately(pa):
+    q = pa.Sched(100, aging_ns=50)
+    assert q.submit(1, 70, 0, lane=0) == OK
+    assert q.submit(2, 10, 0, lane=1) == OK
+    assert q.submit(3, 60, 0, lane=0) == OK
+    assert q.admit(1, lanes=1 << 1) == [2]          # lane 1 only
+    assert q.admit(2, lanes=1 << 0) == [1]          # 3 does not fit
+    assert q.submit(4, 10, 60, lane=1) == OK
+    assert q.submit(5, 10, 60, lane=0) == OK
+    # 3 has aged in lane 0: 5 waits behind it, but lane 1's 4 is not held back
+    assert q.admit(100) == [4]
+    q.release(1)
+    assert q.admit(101) == [3, 5]
+
+
+def _lane_model(budget, aging, ops):
+    queue, held, used, out = [], {}, 0, []
+    for op in ops:
+        if op[0] == "submit":
+            _, t, b, now, lane = op
+            if b > budget:
+                out.append(CAPACITY)
+                continue
+            queue.append((t, b, now, lane))
+            out.append(OK)
+        elif op[0] == "admit":
+            _, now, cap, mask = op
+            got, keep, open_ = [], [], mask
+            for t, b, ts, lane in queue:
+                if len(got) >= cap or not (open_ >> lane) & 1:
+                    keep.append((t, b, ts, lane))
+                elif b <= budget - used:
+                    used += b
+                    held[t] = b
+                    got.append(t)
+                else:
+                    if now - ts >= aging:
+                        open_ &= ~(1 << lane)
+                    keep.append((t, b, ts, lane))
+            queue = keep
+            out.append(got)
+        else:
+            _, t = op
+            used -= held.pop(t)
+            out.append(OK)
+    return out, used
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_lanes_match_policy_model(pa, seed):
+    """The lane rule restated in Python, on random traces over three lanes."""
+    rng = np.random.default_rng(100 + seed)
+    budget, aging = 1000, 40
+    q = pa.Sched(budget, aging_ns=aging)
+    ops, now, next_t, admitted = [], 0, 1, []
+    for _ in range(400):
+        now += int(rng.integers(0, 10))
+        r = rng.random()
+        if r < 0.5:
+            ops.append(("submit", next_t, int(rng.integers(1, 1200)), now, int(rng.integers(0, 3))))
+            next_t += 1
+        elif r < 0.8 or not admitted:
+            ops.append(("admit", now, int(rng.integers(1, 6)), int(rng.integers(1, 8))))
+            res, _ = _lane_model(budget, aging, ops)
+            admitted.extend(res[-1])
+        else:
+            ops.append(("release", admitted.pop(int(rng.integers(0, len(admitted))))))
+    want, used = _lane_model(budget, aging, ops)
+    got = []
+    for op in ops:
+        if op[0] == "submit":
+            got.append(q.submit(op[1], op[2], op[3], lane=op[4]))
+        elif op[0] == "admit":
+            got.append(q.admit(op[1], op[2], lanes=op[3]))
+        else:
+            got.append(q.release(op[1]))
+    assert got == want
+    assert q.in_use == used

@@ -120,7 +120,7 @@ __global__ void seed_out_kernel(uint32_t d, uint32_t seed_mode, uint32_t *seed_o
 // ---------------------------------------------------------------------------
 constexpr uint32_t kRadixThreads = 512, kRadixWarps = kRadixThreads / 32;
 constexpr uint32_t kRadixBuckets = 512;   // the widest digit: 9 bits
-constexpr uint32_t kRadixRounds = 16;     // items per lane per tile
+constexpr uint32_t kRadixRounds = 12;     // items per lane per tile
 constexpr uint32_t kRadixTile = kRadixThreads * kRadixRounds;
 constexpr uint32_t kMaxPasses = 4;
 constexpr unsigned long long kBadKey = 0xffffffffull;   // sorts after every node id
@@ -216,7 +216,7 @@ struct RadixSmem {
 };
 
 template <typename Id, bool First, uint32_t DB>
-__global__ void __launch_bounds__(kRadixThreads, 2) radix_pass_kernel(
+__global__ void __launch_bounds__(kRadixThreads, 3) radix_pass_kernel(
     const void *src, unsigned long long *dst, uint64_t n_items, uint32_t shift, uint64_t n,
     const unsigned long long *digit_base, unsigned long long *status, uint32_t epoch,
     unsigned long long *tile_ctr, uint64_t spin_limit_ns, uint32_t *err)
@@ -240,18 +240,21 @@ __global__ void __launch_bounds__(kRadixThreads, 2) radix_pass_kernel(
     // order (conflict-free); only their digits stay in registers through the
     // ranking and the look-back, which keeps the kernel free of spills
     uint32_t dgp[kRadixRounds / 2];   // two digits per register
-    {
-        unsigned long long its[kRadixRounds];
+    // loaded in two halves: all of a thread's items at once spill registers
 #pragma unroll
-        for (uint32_t r = 0; r < kRadixRounds; ++r) {
-            const uint32_t k = wo + r * 32 + lane;
-            its[r] = k < tcount ? radix_item<Id, First>(src, tb + k, n, err) : 0ull;
+    for (uint32_t h = 0; h < kRadixRounds; h += kRadixRounds / 2) {
+        unsigned long long its[kRadixRounds / 2];
+#pragma unroll
+        for (uint32_t q = 0; q < kRadixRounds / 2; ++q) {
+            const uint32_t k = wo + (h + q) * 32 + lane;
+            its[q] = k < tcount ? radix_item<Id, First>(src, tb + k, n, err) : 0ull;
         }
 #pragma unroll
-        for (uint32_t r = 0; r < kRadixRounds; ++r) {
+        for (uint32_t q = 0; q < kRadixRounds / 2; ++q) {
+            const uint32_t r = h + q;
             const uint32_t k = wo + r * 32 + lane;
-            S.stage[k] = its[r];
-            const uint32_t dg = k < tcount ? (uint32_t)(its[r] >> (32 + shift)) & MASK : NB + lane;
+            S.stage[k] = its[q];
+            const uint32_t dg = k < tcount ? (uint32_t)(its[q] >> (32 + shift)) & MASK : NB + lane;
             if (r & 1) dgp[r / 2] |= dg << 16;
             else dgp[r / 2] = dg;
         }

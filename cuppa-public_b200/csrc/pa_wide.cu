@@ -17,7 +17,10 @@
 //    a final lower lane is redrawn;
 //  * a copy read of slot (v, k) re-reads it while it holds the all-ones fill
 //    (the slot-granular completion of the start kernel: the value is its own
-//    flag), and every slot is stored the moment it is final.
+//    flag), and every slot is stored the moment it is final;
+//  * the first candidate (retry 0) of every slot of the node is drawn and read
+//    before the chunks are resolved (kept in shared memory beside the set, up
+//    to d = 8192), so the chunks' copy reads are in flight together.
 //
 // The draws (Philox counter (u_lo, u_hi, slot, retry)), the slot order and the
 // rejection rule are the start kernel's, so the output is bit-identical to the
@@ -101,14 +104,67 @@ __device__ __forceinline__ void wide_classify(WSlot &s, uint32_t u, uint32_t i, 
     }
 }
 
+// Retry-0 candidates of all of a node's slots, fetched before its chunks are
+// resolved: the draws do not depend on the resolution, so the copy reads of
+// every chunk are in flight together instead of one chunk's at a time.  kPre
+// slots per lane are drawn, then their reads issued, then classified.
+template <typename Id, bool Slots>
+__device__ __forceinline__ void wide_prefetch(uint32_t *pre_val, uint32_t *pre_meta, uint32_t u,
+                                              const GenArgs &a, const Id *E, uint32_t lane,
+                                              uint32_t &n_pend)
+{
+    constexpr uint32_t kPre = 4;
+    const uint32_t d = a.d;
+    for (uint32_t i0 = lane; i0 < d; i0 += 32 * kPre) {
+        DrawT<uint32_t> dr[kPre];
+        uint64_t x[kPre];
+#pragma unroll
+        for (uint32_t q = 0; q < kPre; ++q) {
+            const uint32_t i = i0 + 32 * q;
+            if (i < d) dr[q] = draw<uint32_t>(u, i, 0u, a);
+        }
+#pragma unroll
+        for (uint32_t q = 0; q < kPre; ++q) {
+            const uint32_t i = i0 + 32 * q;
+            x[q] = 0;
+            if (i < d && !dr[q].direct && dr[q].v > d)
+                x[q] = ld_slot(slot_addr<Id, uint32_t, Slots>(E, a, dr[q].v, dr[q].k));
+        }
+#pragma unroll
+        for (uint32_t q = 0; q < kPre; ++q) {
+            const uint32_t i = i0 + 32 * q;
+            if (i >= d) continue;
+            uint32_t val, known = 1u;
+            if (dr[q].direct) {
+                val = dr[q].v;
+            } else if (dr[q].v <= d) {
+                val = (uint32_t)seed_slot(dr[q].v, dr[q].k, d, a.seed_mode);
+            } else if (x[q] != WideSentinel<Id>::value) {
+                val = (uint32_t)x[q];
+            } else {
+                val = dr[q].v;   // pending: polled while its chunk is resolved
+                known = 0u;
+                ++n_pend;
+            }
+            pre_val[i] = val;
+            pre_meta[i] = dr[q].k | (known << 31);
+        }
+    }
+}
+
 template <typename Id, bool Slots>
 __global__ void wide_kernel(const GenArgs a, unsigned long long *ticket, uint32_t cap_log2,
-                            uint32_t write_seeds)
+                            uint32_t write_seeds, uint32_t prefetch)
 {
     extern __shared__ uint32_t wide_smem[];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t cap = 1u << cap_log2;
-    uint32_t *set = wide_smem + (size_t)warp * cap;
+    // per warp: the hash set, then (with prefetch) each slot's retry-0 candidate
+    // and its source slot k with a known bit
+    const size_t warp_words = cap + (prefetch ? 2ull * a.d : 0ull);
+    uint32_t *set = wide_smem + (size_t)warp * warp_words;
+    uint32_t *pre_val = set + cap;
+    uint32_t *pre_meta = pre_val + a.d;
     const uint32_t lt = lanemask_lt(), le = lt | (1u << lane);
     const uint32_t d = a.d;
     Id *E = reinterpret_cast<Id *>(a.edges);
@@ -137,12 +193,20 @@ __global__ void wide_kernel(const GenArgs a, unsigned long long *ticket, uint32_
         const bool withhold = a.withhold_first && row == 0;
         __syncwarp();
         for (uint32_t x = lane; x < cap; x += 32) set[x] = kEmpty;
+        if (prefetch) wide_prefetch<Id, Slots>(pre_val, pre_meta, u, a, E, lane, n_pend);
         __syncwarp();
         for (uint32_t c0 = 0; c0 < d && ok; c0 += 32) {
             const uint32_t i = c0 + lane;
             const bool active = i < d;
             WSlot s{0u, 0u, 0u, true};
-            if (active) wide_classify<Id, Slots>(s, u, i, 0u, a, E, n_pend);
+            if (active && prefetch) {
+                const uint32_t m = pre_meta[i];
+                s.val = pre_val[i];
+                s.k = m & 0x7fffffffu;
+                s.known = (m >> 31) != 0u;
+            } else if (active) {
+                wide_classify<Id, Slots>(s, u, i, 0u, a, E, n_pend);
+            }
             bool stored = !active;
             const uint64_t e = a.seed_edges + row * d + i;
             uint64_t spin_t0 = 0;
@@ -249,7 +313,9 @@ template <typename Id, bool Slots>
 int launch_wide_t(const GenArgs &a, unsigned long long *ticket, uint32_t blocks, cudaStream_t s)
 {
     const uint32_t lg = set_cap_log2(a.d);
-    const size_t warp_bytes = 4ull << lg;
+    // fetch every slot's first candidate up front when it fits beside the set
+    const bool prefetch = (4ull << lg) + 8ull * a.d <= kWideSetMaxBytes;
+    const size_t warp_bytes = (4ull << lg) + (prefetch ? 8ull * a.d : 0ull);
     const uint32_t warps = (uint32_t)std::max<size_t>(
         1, std::min<size_t>(8, kWideBlockSetBytes / warp_bytes));
     const size_t smem = warp_bytes * warps;
@@ -269,7 +335,7 @@ int launch_wide_t(const GenArgs &a, unsigned long long *ticket, uint32_t blocks,
         if (need < g) g = need > 0 ? need : 1;
         blocks = (uint32_t)g;
     }
-    kern<<<blocks, 32 * warps, smem, s>>>(a, ticket, lg, 1u);
+    kern<<<blocks, 32 * warps, smem, s>>>(a, ticket, lg, 1u, prefetch ? 1u : 0u);
     e = cudaGetLastError();
     return e == cudaSuccess ? PA_OK : set_cuda_error(e);
 }

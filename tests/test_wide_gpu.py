@@ -122,3 +122,14 @@ def test_wide_limits(pa, cuda_ok):
     with pa.Server(budget_bytes=1 << 30) as srv:
         rc, _ = srv.try_submit(pa.make_params(1000, 40, 0.5))
         assert rc == pa.PA_ERR_NOT_SUPPORTED
+
+
+def test_wide_wait_limit_reports_error_and_context_survives(pa, cuda_ok):
+    """The first generated node's slots are never stored (a test flag): every
+    copy read of them waits until the 20 ms limit, the call returns
+    PA_ERR_SPIN_TIMEOUT, and the context stays usable."""
+    prm = pa.make_params(20_000, 40, 0.2, seed=1, flags=pa.PA_FLAG_TEST_WITHHOLD_FIRST_TILE,
+                         spin_limit_ns=20_000_000)
+    _, st = pa.generate(prm, raise_on_error=False)
+    assert st.status == pa.PA_ERR_SPIN_TIMEOUT
+    _check(pa, 3000, 40, 0.2, 1, 1, 32)

@@ -179,7 +179,7 @@ __global__ void wide_kernel(const GenArgs a, unsigned long long *ticket, uint32_
         }
     }
 
-    uint32_t n_retry = 0, n_wait = 0, n_pend = 0, n_poll = 0, n_done = 0;
+    uint32_t n_retry = 0, n_wait = 0, n_pend = 0, n_poll = 0;
     const uint32_t max_sleep = min(a.max_sleep_ns, 512u);
     bool ok = true;
     while (ok) {
@@ -281,7 +281,6 @@ __global__ void wide_kernel(const GenArgs a, unsigned long long *ticket, uint32_
             if (ok && active) set_insert(set, cap_log2, s.val);
             __syncwarp();
         }
-        if (ok) ++n_done;
     }
 
 #pragma unroll

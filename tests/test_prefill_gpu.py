@@ -25,3 +25,19 @@ def test_prefilled_generation_equals_plain(pa, cuda_ok, n, d, bits, layout):
     assert pa.finish(scratch).status == 0
     got = edges[: want.shape[0]]
     assert torch.equal(got, want)
+
+
+def test_fill_of_a_seed_only_graph_is_empty(pa, cuda_ok):
+    """n = d + 1 has no generated slots: the fill writes nothing and the
+    prefilled generation still writes the seed edges."""
+    prm = pa.make_params(5, 4, 0.5, seed=1, id_bits=64)
+    edges, scratch = pa.alloc_buffers(prm)
+    edges.fill_(7)
+    pa.fill(prm, edges)
+    torch.cuda.synchronize()
+    assert bool((edges == 7).all())
+    q = pa.make_params(5, 4, 0.5, seed=1, id_bits=64, flags=pa.PA_FLAG_PREFILLED)
+    pa.generate_into(q, edges, scratch)
+    assert pa.finish(scratch).status == 0
+    want, _ = pa.generate(prm)
+    assert torch.equal(edges[: want.shape[0]], want)

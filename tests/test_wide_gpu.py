@@ -133,3 +133,15 @@ def test_wide_wait_limit_reports_error_and_context_survives(pa, cuda_ok):
     _, st = pa.generate(prm, raise_on_error=False)
     assert st.status == pa.PA_ERR_SPIN_TIMEOUT
     _check(pa, 3000, 40, 0.2, 1, 1, 32)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_wide_seed_only_graph(pa, cuda_ok, mode):
+    """n = d + 1: the seed graph alone -- generation, CSR and canonical rows."""
+    d = 40
+    prm, E, G = _check(pa, d + 1, d, 0.5, 3, mode, 32)
+    rowptr, col = pa.build_csr(prm, E)
+    want_rp, want_col = orc.csr(G, mode)
+    assert (rowptr.cpu().numpy() == want_rp).all() and (col.cpu().numpy() == want_col).all()
+    pa.canonicalize(prm, E)
+    assert (E.cpu().numpy() == orc.pairs_canonical(G, mode)).all()

@@ -860,7 +860,8 @@ def measure_served(args, rate: float, seconds: float, outputs_name: str, world: 
     prms = [pa.make_params(r["n"], r["d"], r["p"], seed=r["seed"], id_bits=32,
                            seed_mode=pa.PA_SEED_CLIQUE) for r in reqs]
     tickets = queue.Queue()
-    lat, edges_done, statuses = [], 0, []
+    lat, edges_done, statuses, small = [], 0, [], []
+    express_edges = args.serve_express_edges or (1 << 22)   # the server's default
     outputs = {"pairs": pa.PA_OUT_PAIRS, "csr": pa.PA_OUT_CSR,
                "both": pa.PA_OUT_PAIRS | pa.PA_OUT_CSR}[outputs_name]
     with pa.Server(budget_bytes=budget, outputs=outputs, max_inflight=args.serve_max_inflight,
@@ -894,6 +895,7 @@ def measure_served(args, rate: float, seconds: float, outputs_name: str, world: 
             rc, res = srv.wait(t)
             statuses.append(res.status if rc == 0 else rc)
             lat.append((res.t_done_ns - res.t_submit_ns) / 1e6)
+            small.append(res.n_edges <= express_edges)
             first_submit = res.t_submit_ns if first_submit is None else min(first_submit,
                                                                            res.t_submit_ns)
             last_done = max(last_done, res.t_done_ns)
@@ -907,8 +909,9 @@ def measure_served(args, rate: float, seconds: float, outputs_name: str, world: 
     if world > 1:
         span_s = max_over_ranks(span_s, world, "cuda")
         gathered = [None] * world
-        dist.all_gather_object(gathered, (lat, edges_done, ok, n_req))
+        dist.all_gather_object(gathered, (lat, edges_done, ok, n_req, small))
         lat = [x for g in gathered for x in g[0]]
+        small = [x for g in gathered for x in g[4]]
         edges_done = sum(g[1] for g in gathered)
         ok = all(g[2] for g in gathered)
         n_req = sum(g[3] for g in gathered)
@@ -916,6 +919,13 @@ def measure_served(args, rate: float, seconds: float, outputs_name: str, world: 
 
     def pct(x):
         return lat_sorted[min(len(lat_sorted) - 1, int(round(x / 100 * (len(lat_sorted) - 1))))]
+
+    def pcts(sel):
+        v = sorted(x for x, m in zip(lat, small) if m == sel)
+        if not v:
+            return None
+        return {"requests": len(v), "p50_ms": v[len(v) // 2],
+                "p99_ms": v[min(len(v) - 1, int(round(0.99 * (len(v) - 1))))]}
 
     offered_edges = sum(edges_of(r["n"], r["d"]) for r in all_reqs)
     fig = {
@@ -928,6 +938,7 @@ def measure_served(args, rate: float, seconds: float, outputs_name: str, world: 
         "offered_requests_per_s": rate, "offered_edges_per_s": offered_edges / seconds,
         "served_requests_per_s": n_req / span_s, "edges_per_s": edges_done / span_s,
         "span_s": span_s, "p50_ms": pct(50), "p99_ms": pct(99), "max_ms": lat_sorted[-1],
+        "express_sized": pcts(True), "bulk_sized": pcts(False),
         "all_ok": ok, "server_stats_rank0": st,
         "statuses_rank0": {str(c): statuses.count(c) for c in sorted(set(statuses))},
         "gpu_launches": st["batches"] * 2 + (st["completed"] * 11 if outputs & pa.PA_OUT_CSR else 0),

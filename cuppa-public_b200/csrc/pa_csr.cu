@@ -23,6 +23,7 @@
 // look-back (Merrill and Garland's single-pass prefix scan, as in Adinets and
 // Merrill's one-sweep radix sort) instead of a per-pass histogram and scan.
 #include <algorithm>
+#include <limits>
 #include <type_traits>
 #include <vector>
 
@@ -405,13 +406,13 @@ __global__ void seed_prefix_kernel(const uint32_t *seed_out, uint32_t d, int64_t
     }
 }
 
-// One pass over the sorted items: in part entry i (key v, value u) goes to
-// col[outprefix(v + 1) + i], and rowptr[x] = outprefix(x) + #items with key < x
+// One pass over the sorted items: rowptr[x] = outprefix(x) + #items with key < x
 // is written for every x in (key(i-1), key(i)] (i = n_items closes the range up
-// to n; keys >= n -- only after an input error -- count as n).  Consecutive
-// threads take consecutive items (coalesced stores); a thread's U items of one
-// step are a grid stride apart, their loads issued together.
-template <typename Id>
+// to n; keys >= n -- only after an input error -- count as n), and with WriteCol
+// in part entry i (key v, value u) goes to col[outprefix(v + 1) + i].
+// Consecutive threads take consecutive items (coalesced stores); a thread's U
+// items of one step are a grid stride apart, their loads issued together.
+template <typename Id, bool WriteCol>
 __global__ void in_sorted_kernel(const unsigned long long *items, uint64_t n_items, uint64_t n,
                                  uint32_t d, uint64_t seed_edges, const int64_t *seed_pre, Id *col,
                                  uint64_t col_len, int64_t *rowptr)
@@ -435,12 +436,209 @@ __global__ void in_sorted_kernel(const unsigned long long *items, uint64_t n_ite
             const uint64_t lo = i > 0 ? min((uint64_t)(pv[q] >> 32), n) + 1 : 0;
             for (uint64_t x = lo; x <= v && x <= n; ++x)
                 rowptr[x] = (int64_t)(outprefix(x, d, seed_edges, seed_pre) + i);
-            if (i < n_items && v < n) {
+            if (WriteCol && i < n_items && v < n) {
                 const uint64_t pos = outprefix(v + 1, d, seed_edges, seed_pre) + i;
                 if (pos < col_len) col[pos] = (Id)(it[q] & 0xffffffffull);
             }
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Whole rows (d <= 32), once rowptr is known: a warp writes 32 consecutive rows,
+// each out part then in part, so every 32-byte sector of col between the
+// chunk's first and last entry is written by one warp within a short time.
+// (Out parts and in parts written by two kernels share a partial sector at
+// every row boundary, which DRAM then reads and writes back twice.)
+//
+// Row x's in part is sorted items [lb(x), lb(x+1)), lb(x) = rowptr[x] -
+// outprefix(x); entry k of it (item index) goes to col[outprefix(x+1) + k].
+// A row whose in part is longer than kHeavyIn items is left to
+// heavy_in_kernel (listed here), so that hub rows do not hold one warp.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kRowsChunk = 32;        // rows per warp step: one per lane
+constexpr uint64_t kHeavyIn = 512;         // longest in part a row warp copies
+constexpr uint64_t kGiantIn = 1ull << 20;  // longer: copied by the whole grid
+
+__device__ __forceinline__ uint64_t clamp_items(int64_t v, uint64_t n_items)
+{
+    return v < 0 ? 0ull : ((uint64_t)v > n_items ? n_items : (uint64_t)v);
+}
+
+// Out degree of row x: seed rows from the prefix table, d for the others.
+__device__ __forceinline__ uint32_t outdeg(uint64_t x, uint32_t d, const int64_t *seed_pre)
+{
+    return x <= (uint64_t)d ? (uint32_t)(seed_pre[x + 1] - seed_pre[x]) : d;
+}
+
+// Copy sorted items [a, b) (all of key v or, in a row warp, of keys in the
+// warp's rows) into their in part places; U loads per lane in flight.
+template <typename Id>
+__device__ __forceinline__ void copy_in_items(const unsigned long long *items, uint64_t a, uint64_t b,
+                                              uint32_t lane, uint64_t n, uint32_t d,
+                                              uint64_t seed_edges, const int64_t *seed_pre, Id *col,
+                                              uint64_t col_len)
+{
+    constexpr uint32_t U = 4;
+    for (uint64_t k0 = a; k0 < b; k0 += 32 * U) {
+        unsigned long long it[U];
+#pragma unroll
+        for (uint32_t q = 0; q < U; ++q) {
+            const uint64_t k = k0 + q * 32 + lane;
+            it[q] = k < b ? items[k] : ~0ull;
+        }
+#pragma unroll
+        for (uint32_t q = 0; q < U; ++q) {
+            const uint64_t k = k0 + q * 32 + lane;
+            const uint64_t v = it[q] >> 32;
+            if (k < b && v < n) {
+                const uint64_t pos = outprefix(v + 1, d, seed_edges, seed_pre) + k;
+                if (pos < col_len) col[pos] = (Id)(it[q] & 0xffffffffull);
+            }
+        }
+    }
+}
+
+template <typename Id>
+__global__ void __launch_bounds__(256) rows_kernel(const Id *E, const unsigned long long *items,
+                                                   uint64_t n_items, const int64_t *rowptr, Id *col,
+                                                   uint64_t n, uint32_t d, uint64_t seed_edges,
+                                                   const int64_t *seed_pre, uint64_t col_len,
+                                                   unsigned long long *heavy, uint64_t heavy_cap,
+                                                   unsigned long long *giant, uint64_t giant_cap,
+                                                   unsigned long long *ctr)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    const uint64_t w0 = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint32_t G = 32u / d;   // rows per out part pass, d lanes each
+    const uint32_t g = lane / d, i = lane - g * d;
+    const bool used = lane < G * d;
+    for (uint64_t x0 = w0 * kRowsChunk; x0 < n; x0 += warps * kRowsChunk) {
+        // lane j: row x0 + j, its rowptr and its in part's item range
+        const uint64_t x = x0 + lane;
+        const bool row_ok = x < n;
+        int64_t rp = 0;
+        uint64_t lb = n_items, lb1 = n_items;
+        if (row_ok) {
+            rp = rowptr[x];
+            const int64_t rp1 = rowptr[x + 1];
+            lb = clamp_items(rp - (int64_t)outprefix(x, d, seed_edges, seed_pre), n_items);
+            lb1 = clamp_items(rp1 - (int64_t)outprefix(x + 1, d, seed_edges, seed_pre), n_items);
+            if (lb1 < lb) lb1 = lb;
+        }
+        const bool heavy_row = row_ok && lb1 - lb > kHeavyIn;
+        if (heavy_row) {
+            // listed in any order: every entry's place is fixed by its index
+            if (lb1 - lb > kGiantIn) {
+                const unsigned long long s = atomicAdd(ctr + 1, 1ull);
+                if (s < giant_cap) giant[s] = x;
+            } else {
+                const unsigned long long s = atomicAdd(ctr, 1ull);
+                if (s < heavy_cap) heavy[s] = x;
+            }
+        }
+
+        // (a) out parts, G rows per pass, each row's d targets ranked in
+        // registers; U passes' loads issued together.  Seed rows hold targets
+        // 0, 1, ... (both seed graphs); their absent slots sort last.
+        constexpr uint32_t U = 4;
+        for (uint32_t r0 = 0; r0 < kRowsChunk; r0 += U * G) {
+            Id t[U];
+            bool have[U];
+            int64_t rrp[U];
+#pragma unroll
+            for (uint32_t q = 0; q < U; ++q) {
+                const uint32_t rj = r0 + q * G + g;
+                rrp[q] = __shfl_sync(kFull, rp, rj & 31u);
+                const uint64_t row = x0 + rj;
+                const bool act = used && rj < kRowsChunk && row < n;
+                t[q] = std::numeric_limits<Id>::max();
+                have[q] = false;
+                if (act && row > d) {
+                    t[q] = E[2 * (seed_edges + (row - d - 1) * d + i) + 1];
+                    have[q] = true;
+                } else if (act && i < outdeg(row, d, seed_pre)) {
+                    t[q] = (Id)i;
+                    have[q] = true;
+                }
+            }
+#pragma unroll
+            for (uint32_t q = 0; q < U; ++q) {
+                uint32_t rank = 0;
+                for (uint32_t j = 0; j < d; ++j) {
+                    const Id o = __shfl_sync(kFull, t[q], (g * d + j) & 31u);
+                    rank += (o < t[q]) ? 1u : 0u;
+                }
+                if (have[q]) {
+                    const uint64_t pos = (uint64_t)rrp[q] + rank;
+                    if (pos < col_len) col[pos] = t[q];
+                }
+            }
+        }
+
+        // (b) in parts of the chunk's rows, the heavy rows' ranges skipped
+        uint32_t hv = __ballot_sync(kFull, heavy_row);
+        uint64_t a = __shfl_sync(kFull, lb, 0);
+        const uint64_t end = __shfl_sync(kFull, lb1, 31);
+        while (true) {
+            uint64_t b = end, next = end;
+            if (hv) {
+                const uint32_t h = __ffs(hv) - 1;
+                b = __shfl_sync(kFull, lb, h);
+                next = __shfl_sync(kFull, lb1, h);
+                hv &= hv - 1;
+            }
+            if (b > a) copy_in_items(items, a, b, lane, n, d, seed_edges, seed_pre, col, col_len);
+            if (b == end && next == end) break;
+            a = next;
+        }
+    }
+}
+
+// In parts of the listed rows: a heavy row per block (block stride over the
+// list), then each giant row by the whole grid.
+template <typename Id>
+__global__ void __launch_bounds__(256) heavy_in_kernel(const unsigned long long *items,
+                                                       uint64_t n_items, const int64_t *rowptr,
+                                                       Id *col, uint64_t n, uint32_t d,
+                                                       uint64_t seed_edges, const int64_t *seed_pre,
+                                                       uint64_t col_len,
+                                                       const unsigned long long *heavy,
+                                                       uint64_t heavy_cap,
+                                                       const unsigned long long *giant,
+                                                       uint64_t giant_cap,
+                                                       const unsigned long long *ctr)
+{
+    const uint64_t n_heavy = min((uint64_t)ctr[0], heavy_cap);
+    const uint64_t n_giant = min((uint64_t)ctr[1], giant_cap);
+    auto copy_row = [&](uint64_t x, uint64_t first, uint64_t stride) {
+        if (x >= n) return;
+        const uint64_t lb = clamp_items(rowptr[x] - (int64_t)outprefix(x, d, seed_edges, seed_pre),
+                                        n_items);
+        const uint64_t lb1 = clamp_items(
+            rowptr[x + 1] - (int64_t)outprefix(x + 1, d, seed_edges, seed_pre), n_items);
+        const uint64_t base = outprefix(x + 1, d, seed_edges, seed_pre);
+        constexpr uint32_t U = 4;
+        for (uint64_t k0 = lb + first; k0 < lb1; k0 += U * stride) {
+            unsigned long long it[U];
+#pragma unroll
+            for (uint32_t q = 0; q < U; ++q) {
+                const uint64_t k = k0 + q * stride;
+                it[q] = k < lb1 ? items[k] : 0ull;
+            }
+#pragma unroll
+            for (uint32_t q = 0; q < U; ++q) {
+                const uint64_t k = k0 + q * stride, pos = base + k;
+                if (k < lb1 && pos < col_len) col[pos] = (Id)(it[q] & 0xffffffffull);
+            }
+        }
+    };
+    for (uint64_t h = blockIdx.x; h < n_heavy; h += gridDim.x)
+        copy_row(heavy[h], threadIdx.x, blockDim.x);
+    const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (uint64_t h = 0; h < n_giant; ++h)
+        copy_row(giant[h], gt, (uint64_t)gridDim.x * blockDim.x);
 }
 
 int grid_for(uint64_t items, uint32_t threads, uint32_t per_sm = 8)
@@ -455,8 +653,9 @@ int grid_for(uint64_t items, uint32_t threads, uint32_t per_sm = 8)
 
 struct CsrLayout {
     uint64_t items_off, status_off, hist_off, base_off, ctr_off, err_off, seed_out_off,
-        seed_pre_off, total;
-    uint64_t r_tiles;   // radix tiles
+        seed_pre_off, heavy_off, giant_off, total;
+    uint64_t r_tiles;               // radix tiles
+    uint64_t heavy_cap, giant_cap;  // rows with in parts above kHeavyIn / kGiantIn items
 };
 
 // Graphs below 2^32 nodes: items pack (v, u) in 8 bytes.
@@ -473,10 +672,15 @@ CsrLayout csr_layout(uint64_t n, uint32_t d, uint64_t n_edges)
     L.status_off = o;   o += al(8 * kRadixBuckets * std::max<uint64_t>(L.r_tiles, 1));
     L.hist_off = o;     o += al(8 * kMaxPasses * kRadixBuckets);
     L.base_off = o;     o += al(8 * kMaxPasses * kRadixBuckets);
-    L.ctr_off = o;      o += 256;   // one tile counter per pass
+    L.ctr_off = o;      o += 256;   // one tile counter per pass, then the two row lists'
     L.err_off = o;      o += 256;
     L.seed_out_off = o; o += al(4 * (d + 1));
     L.seed_pre_off = o; o += al(8 * (d + 2));
+    // more than cap rows cannot each hold more than kHeavyIn of the n_edges items
+    L.heavy_cap = n_edges / (kHeavyIn + 1) + 1;
+    L.giant_cap = n_edges / (kGiantIn + 1) + 1;
+    L.heavy_off = o;    o += al(8 * L.heavy_cap);
+    L.giant_off = o;    o += al(8 * L.giant_cap);
     L.total = o;
     return L;
 }
@@ -553,14 +757,31 @@ int csr_enqueue_t(const pa_params *prm, const GenPlan &p, const Id *E, int64_t *
         if (rc != PA_OK) return rc;
     }
     const uint64_t col_len = 2 * m;
-    in_sorted_kernel<Id><<<grid_for(m / 4 + 1, 256), 256, 0, s>>>(A, m, n, d, p.seed_edges,
-                                                                   seed_pre, col, col_len, rowptr);
-    out_part_kernel<Id><<<grid_for(n * d / 4 + 1, 256), 256, 0, s>>>(E, rowptr, col, n, d,
-                                                                     p.seed_edges, col_len);
     if (p.wide) {
-        // the generated rows of d > 32 (out_part_kernel wrote the seed rows)
+        // in parts and rowptr from the sorted items, the seed rows' out parts,
+        // then the generated rows' out parts (ranked in shared memory)
+        in_sorted_kernel<Id, true><<<grid_for(m / 4 + 1, 256), 256, 0, s>>>(
+            A, m, n, d, p.seed_edges, seed_pre, col, col_len, rowptr);
+        out_part_kernel<Id><<<grid_for(n * d / 4 + 1, 256), 256, 0, s>>>(E, rowptr, col, n, d,
+                                                                         p.seed_edges, col_len);
         const int rc = gen::csr_out_wide(p.id_bytes, E, rowptr, col, n, d, p.seed_edges, col_len, s);
         if (rc != PA_OK) return rc;
+    } else {
+        // rowptr, then whole rows (the hub rows' in parts listed and copied last)
+        unsigned long long *lists = (unsigned long long *)(scratch + L.ctr_off) + kMaxPasses;
+        unsigned long long *heavy = (unsigned long long *)(scratch + L.heavy_off);
+        unsigned long long *giant = (unsigned long long *)(scratch + L.giant_off);
+        e = cudaMemsetAsync(lists, 0, 16, s);
+        if (e != cudaSuccess) return set_cuda_error(e);
+        in_sorted_kernel<Id, false><<<grid_for(m / 4 + 1, 256), 256, 0, s>>>(
+            A, m, n, d, p.seed_edges, seed_pre, col, col_len, rowptr);
+        const int grid = grid_for(n / kRowsChunk + 1, 256 / 32);
+        rows_kernel<Id><<<grid, 256, 0, s>>>(E, A, m, rowptr, col, n, d, p.seed_edges, seed_pre,
+                                             col_len, heavy, L.heavy_cap, giant, L.giant_cap,
+                                             lists);
+        heavy_in_kernel<Id><<<grid_for(m / 8 + 1, 256), 256, 0, s>>>(
+            A, m, rowptr, col, n, d, p.seed_edges, seed_pre, col_len, heavy, L.heavy_cap, giant,
+            L.giant_cap, lists);
     }
     e = cudaGetLastError();
     return e == cudaSuccess ? PA_OK : set_cuda_error(e);

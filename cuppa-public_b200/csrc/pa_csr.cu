@@ -13,17 +13,18 @@
 //   3. in part entries: sorted item i with destination v goes to position
 //      outprefix(v + 1) + i;
 //   4. out part: each generated row's d targets ranked in registers and stored;
-//      the seed rows' targets come from the (canonical) seed edges.
+//      the seed rows' targets are 0, 1, ... (both seed graphs).
+// Steps 3 and 4 run in one row writer for d <= 32 (a warp writes 32 whole
+// rows), with the in parts of hub rows copied by a block or the whole grid.
 // Items pack (v, u) in 8 bytes, so graphs of 2^32 nodes and more are refused.
 //
 // The sort reads the pairs twice and the items twice per pass: one histogram
 // kernel counts the digits of every pass while reading the pairs once, and each
-// pass is one kernel that keeps its tile's items in registers from the load to
-// the store, taking each digit's offset from the tiles before it by decoupled
+// pass is one kernel that keeps its tile on chip from the load to the store,
+// taking each digit's offset from the tiles before it by decoupled
 // look-back (Merrill and Garland's single-pass prefix scan, as in Adinets and
 // Merrill's one-sweep radix sort) instead of a per-pass histogram and scan.
 #include <algorithm>
-#include <limits>
 #include <type_traits>
 #include <vector>
 
@@ -107,20 +108,20 @@ __global__ void seed_out_kernel(uint32_t d, uint32_t seed_mode, uint32_t *seed_o
 // goes to col[outprefix(v + 1) + i], where outprefix(x) is the number of out
 // entries of rows below x -- a closed form -- and rowptr[x] = outprefix(x) +
 // (number of items with key < x), read off the run boundaries.  No atomics on
-// the node range, no per-row sorting, no special path for hub rows.
+// the node range and no per-row sorting.
 //
-// A pass sorts 8 or 9 key bits.  Its kernel claims tiles of 8192 items in
-// order from a counter; a tile's 512 threads load 16 items each into
-// registers, rank them stably -- each of 16 warps walks its 512 items in
-// order, 32 at a time, with __match_any_sync for equal digits and 16-bit
-// per-warp counters in shared memory -- publish the tile's count of every
-// digit, and look back over the tiles before it (their counts, or the running
-// total the nearest finished one published) for each digit's global offset.
-// The tile is then staged in shared memory in digit order and every digit's
-// run is written contiguously.
+// A pass sorts 8 or 9 key bits (the fewest passes for the key).  Its
+// kernel claims tiles of 6144 items in order from a counter; a tile's 512
+// threads load 12 items each and park them in shared memory, rank them stably
+// -- each of 16 warps walks its 384 items in order, 32 at a time, with
+// __match_any_sync for equal digits and 16-bit per-warp counters in shared
+// memory -- publish the tile's count of every digit, and look back over the
+// tiles before it (their counts, or the running total the nearest finished
+// one published) for each digit's global offset.  The tile is then staged in
+// shared memory in digit order and every digit's run is written contiguously.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kRadixThreads = 512, kRadixWarps = kRadixThreads / 32;
-constexpr uint32_t kRadixBuckets = 512;   // the widest digit: 9 bits
+constexpr uint32_t kRadixBuckets = 512;   // the widest digit in use: 9 bits
 constexpr uint32_t kRadixRounds = 12;     // items per lane per tile
 constexpr uint32_t kRadixTile = kRadixThreads * kRadixRounds;
 constexpr uint32_t kMaxPasses = 4;
@@ -216,18 +217,22 @@ struct RadixSmem {
     unsigned long long tile;
 };
 
+// Three CTAs per SM up to 9-bit digits; two with the larger 10-bit counters.
 template <typename Id, bool First, uint32_t DB>
-__global__ void __launch_bounds__(kRadixThreads, 3) radix_pass_kernel(
+__global__ void __launch_bounds__(kRadixThreads, DB > 9 ? 2 : 3) radix_pass_kernel(
     const void *src, unsigned long long *dst, uint64_t n_items, uint32_t shift, uint64_t n,
     const unsigned long long *digit_base, unsigned long long *status, uint32_t epoch,
     unsigned long long *tile_ctr, uint64_t spin_limit_ns, uint32_t *err)
 {
     constexpr uint32_t NB = 1u << DB, MASK = NB - 1;
-    static_assert(NB <= kRadixThreads, "one digit per thread");
+    // digits per thread in the per-digit steps (10-bit digits: two)
+    constexpr uint32_t DPT = NB > kRadixThreads ? NB / kRadixThreads : 1;
+    static_assert(NB <= kRadixBuckets && DPT * kRadixThreads >= NB, "digit width");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     RadixSmem<NB> &S = *reinterpret_cast<RadixSmem<NB> *>(smem_raw);
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
     const uint32_t lt = lanemask_lt();
+    const bool owner = tid * DPT < NB;
     for (uint32_t w = 0; w < kRadixWarps; ++w)
         for (uint32_t b = tid; b < NB; b += kRadixThreads) S.wcnt[w][b] = 0;
     if (tid == 0) S.tile = atomicAdd(tile_ctr, 1ull);
@@ -285,54 +290,79 @@ __global__ void __launch_bounds__(kRadixThreads, 3) radix_pass_kernel(
     }
     __syncthreads();
 
-    // 2. thread j owns digit j: its warps' bases in warp order and its count in
-    // the tile, published for the tiles after this one
-    uint32_t tot = 0;
-    if (tid < NB) {
-        for (uint32_t w = 0; w < kRadixWarps; ++w) {
-            const uint32_t c = S.wcnt[w][tid];
-            S.wcnt[w][tid] = (uint16_t)tot;
-            tot += c;
+    // 2. thread j owns digits j*DPT .. j*DPT+DPT-1: their warps' bases in warp
+    // order and their counts in the tile, published for the tiles after this one
+    uint32_t tot[DPT];
+#pragma unroll
+    for (uint32_t j = 0; j < DPT; ++j) {
+        tot[j] = 0;
+        if (owner) {
+            const uint32_t dig = tid * DPT + j;
+            for (uint32_t w = 0; w < kRadixWarps; ++w) {
+                const uint32_t c = S.wcnt[w][dig];
+                S.wcnt[w][dig] = (uint16_t)tot[j];
+                tot[j] += c;
+            }
         }
     }
     const unsigned long long ep = (unsigned long long)epoch << kLbEpochShift;
-    unsigned long long before = 0;   // this digit's items in the tiles before t
-    if (tid < NB) {
-        unsigned long long *mine = status + t * NB + tid;
-        if (t == 0) {
-            st_relaxed_u64(mine, kLbInc | ep | tot);
-        } else {
-            st_relaxed_u64(mine, kLbAgg | ep | tot);
+    unsigned long long before[DPT];   // each digit's items in the tiles before t
+#pragma unroll
+    for (uint32_t j = 0; j < DPT; ++j) before[j] = 0;
+    if (owner) {
+        unsigned long long *mine = status + t * NB + tid * DPT;
+#pragma unroll
+        for (uint32_t j = 0; j < DPT; ++j)
+            st_relaxed_u64(mine + j, (t == 0 ? kLbInc : kLbAgg) | ep | tot[j]);
+        if (t > 0) {
             // 3. look back: add the counts of earlier tiles until one of them
             // carries its running total (bounded wait on tiles not yet ranked).
-            // kLbWindow predecessors are read at once: one at a time, the
-            // running totals would advance one tile per L2 round trip, far
-            // slower than tiles are ranked.
-            uint64_t p = t;   // tiles [p, t) are accounted for
-            const uint64_t t0 = globaltimer_ns();
-            bool done = false;
-            while (!done && p > 0) {
-                unsigned long long w[kLbWindow];
+            // kLbWindow predecessors of each owned digit are read at once: one
+            // at a time, the running totals would advance one tile per L2
+            // round trip, far slower than tiles are ranked.
+            uint64_t p[DPT];   // tiles [p, t) are accounted for
+            bool done[DPT];
 #pragma unroll
-                for (uint32_t k = 0; k < kLbWindow; ++k)
-                    w[k] = k < p ? ld_relaxed_u64(status + (p - 1 - k) * NB + tid) : 0ull;
-                uint32_t used = 0;
+            for (uint32_t j = 0; j < DPT; ++j) {
+                p[j] = t;
+                done[j] = false;
+            }
+            const uint64_t t0 = globaltimer_ns();
+            while (true) {
+                bool open = false;
+#pragma unroll
+                for (uint32_t j = 0; j < DPT; ++j) open |= !done[j] && p[j] > 0;
+                if (!open) break;
+                unsigned long long w[DPT][kLbWindow];
+#pragma unroll
+                for (uint32_t j = 0; j < DPT; ++j)
+#pragma unroll
+                    for (uint32_t k = 0; k < kLbWindow; ++k)
+                        w[j][k] = !done[j] && k < p[j]
+                                      ? ld_relaxed_u64(status + (p[j] - 1 - k) * NB + tid * DPT + j)
+                                      : 0ull;
                 bool waiting = false;
 #pragma unroll
-                for (uint32_t k = 0; k < kLbWindow; ++k) {
-                    if (done || waiting || k >= p) continue;
-                    const bool ready =
-                        (w[k] >> 62) != 0 && ((w[k] >> kLbEpochShift) & 63ull) == epoch;
-                    if (!ready) {
-                        waiting = true;
-                        continue;
+                for (uint32_t j = 0; j < DPT; ++j) {
+                    uint32_t used = 0;
+                    bool stop = done[j];
+#pragma unroll
+                    for (uint32_t k = 0; k < kLbWindow; ++k) {
+                        if (stop || k >= p[j]) continue;
+                        const bool ready = (w[j][k] >> 62) != 0 &&
+                                           ((w[j][k] >> kLbEpochShift) & 63ull) == epoch;
+                        if (!ready) {
+                            waiting = true;
+                            stop = true;
+                            continue;
+                        }
+                        before[j] += w[j][k] & kLbValMask;
+                        ++used;
+                        if ((w[j][k] >> 62) == 2) done[j] = stop = true;
                     }
-                    before += w[k] & kLbValMask;
-                    ++used;
-                    if ((w[k] >> 62) == 2) done = true;
+                    p[j] -= used;
                 }
-                p -= used;
-                if (waiting && !done) {
+                if (waiting) {
                     if (globaltimer_ns() - t0 > spin_limit_ns) {
                         atomicCAS(err, 0u, (uint32_t)PA_ERR_SPIN_TIMEOUT);
                         break;
@@ -340,11 +370,17 @@ __global__ void __launch_bounds__(kRadixThreads, 3) radix_pass_kernel(
                     __nanosleep(32);
                 }
             }
-            st_relaxed_u64(mine, kLbInc | ep | (before + tot));
+#pragma unroll
+            for (uint32_t j = 0; j < DPT; ++j)
+                st_relaxed_u64(mine + j, kLbInc | ep | (before[j] + tot[j]));
         }
     }
-    // 4. digit starts within the tile (exclusive scan of the counts over digits)
-    uint32_t x = tot;
+    // 4. digit starts within the tile (exclusive scan of the counts over
+    // digits: within the thread, then over threads)
+    uint32_t mysum = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < DPT; ++j) mysum += tot[j];
+    uint32_t x = mysum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t y = __shfl_up_sync(kFull, x, o);
@@ -352,14 +388,19 @@ __global__ void __launch_bounds__(kRadixThreads, 3) radix_pass_kernel(
     }
     if (lane == 31) S.wsum[warp] = x;
     __syncthreads();
-    uint32_t start = x - tot;
+    uint32_t start = x - mysum;
     for (uint32_t w = 0; w < warp; ++w) start += S.wsum[w];
-    if (tid < NB) {
-        for (uint32_t w = 0; w < kRadixWarps; ++w)   // <= tile size: fits 16 bits
-            S.wcnt[w][tid] = (uint16_t)(S.wcnt[w][tid] + start);
-        // the digit's global start less its start in the tile (the tile's items
-        // of smaller digits are counted in digit_base, so this is >= 0)
-        S.goff[tid] = digit_base[tid] + before - start;
+    if (owner) {
+#pragma unroll
+        for (uint32_t j = 0; j < DPT; ++j) {
+            const uint32_t dig = tid * DPT + j;
+            for (uint32_t w = 0; w < kRadixWarps; ++w)   // <= tile size: fits 16 bits
+                S.wcnt[w][dig] = (uint16_t)(S.wcnt[w][dig] + start);
+            // the digit's global start less its start in the tile (the tile's
+            // items of smaller digits are counted in digit_base, so this is >= 0)
+            S.goff[dig] = digit_base[dig] + before[j] - start;
+            start += tot[j];
+        }
     }
     __syncthreads();
     // 5. the tile back from its parking place, then into the stage in digit order
@@ -406,13 +447,14 @@ __global__ void seed_prefix_kernel(const uint32_t *seed_out, uint32_t d, int64_t
     }
 }
 
-// One pass over the sorted items: rowptr[x] = outprefix(x) + #items with key < x
-// is written for every x in (key(i-1), key(i)] (i = n_items closes the range up
-// to n; keys >= n -- only after an input error -- count as n), and with WriteCol
-// in part entry i (key v, value u) goes to col[outprefix(v + 1) + i].
+// One pass over the sorted items (the path of d > 32): rowptr[x] = outprefix(x)
+// + #items with key < x is written for every x in (key(i-1), key(i)] (i =
+// n_items closes the range up to n; keys >= n -- only after an input error --
+// count as n), and in part entry i (key v, value u) goes to
+// col[outprefix(v + 1) + i].
 // Consecutive threads take consecutive items (coalesced stores); a thread's U
 // items of one step are a grid stride apart, their loads issued together.
-template <typename Id, bool WriteCol>
+template <typename Id>
 __global__ void in_sorted_kernel(const unsigned long long *items, uint64_t n_items, uint64_t n,
                                  uint32_t d, uint64_t seed_edges, const int64_t *seed_pre, Id *col,
                                  uint64_t col_len, int64_t *rowptr)
@@ -436,10 +478,60 @@ __global__ void in_sorted_kernel(const unsigned long long *items, uint64_t n_ite
             const uint64_t lo = i > 0 ? min((uint64_t)(pv[q] >> 32), n) + 1 : 0;
             for (uint64_t x = lo; x <= v && x <= n; ++x)
                 rowptr[x] = (int64_t)(outprefix(x, d, seed_edges, seed_pre) + i);
-            if (WriteCol && i < n_items && v < n) {
+            if (i < n_items && v < n) {
                 const uint64_t pos = outprefix(v + 1, d, seed_edges, seed_pre) + i;
                 if (pos < col_len) col[pos] = (Id)(it[q] & 0xffffffffull);
             }
+        }
+    }
+}
+
+// rowptr alone (the row writer's input): rowptr[x] = outprefix(x) + the first
+// position k in [0, n_items] whose key is >= x (key(n_items) = n; keys >= n,
+// only after an input error, count as n).  A warp takes 32 * U consecutive
+// positions; for each 32 of them it writes rows (key(k0 - 1), key(k0 + 31)]
+// one per lane, each from the first lane whose key reaches it (a five-step
+// search over the lanes' keys), so a run of rows without in-edges costs one
+// coalesced store per row instead of a loop in one lane.
+__global__ void __launch_bounds__(256) rowptr_kernel(const unsigned long long *items, uint64_t n_items,
+                                                     uint64_t n, uint32_t d, uint64_t seed_edges,
+                                                     const int64_t *seed_pre, int64_t *rowptr)
+{
+    constexpr uint32_t U = 8;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    const uint64_t w0 = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint64_t positions = n_items + 1;
+    // keys, rows and the search in 32 bits (n < 2^32); rows beyond key(k) are
+    // never written by the lane of k
+    const uint32_t n32 = (uint32_t)n;
+    for (uint64_t c0 = w0 * 32 * U; c0 < positions; c0 += warps * 32 * U) {
+        uint32_t key[U];
+#pragma unroll
+        for (uint32_t q = 0; q < U; ++q) {
+            const uint64_t k = c0 + q * 32 + lane;
+            key[q] = k < n_items ? (uint32_t)min(items[k] >> 32, (unsigned long long)n) : n32;
+        }
+        // the first row not yet written: rows up to key(c0 - 1) belong to the
+        // warp holding position c0 - 1
+        uint64_t nxt = c0 == 0 ? 0 : min(items[c0 - 1] >> 32, (unsigned long long)n) + 1;
+#pragma unroll
+        for (uint32_t q = 0; q < U; ++q) {
+            const uint64_t kb = c0 + q * 32;
+            if (kb >= positions) break;   // warp-uniform
+            const uint32_t v = key[q];
+            const uint32_t last = __shfl_sync(kFull, v, 31);
+            for (uint64_t x0 = nxt; x0 <= last; x0 += 32) {
+                const uint64_t x = x0 + lane;
+                const uint32_t xs = (uint32_t)min(x, (uint64_t)last);
+                uint32_t lo = 0;   // lanes whose key is below x
+#pragma unroll
+                for (uint32_t step = 16; step > 0; step >>= 1)
+                    if (__shfl_sync(kFull, v, lo + step - 1) < xs) lo += step;
+                if (x <= last)
+                    rowptr[x] = (int64_t)(outprefix(x, d, seed_edges, seed_pre) + kb + lo);
+            }
+            if ((uint64_t)last + 1 > nxt) nxt = (uint64_t)last + 1;
         }
     }
 }
@@ -540,11 +632,12 @@ __global__ void __launch_bounds__(256) rows_kernel(const Id *E, const unsigned l
         }
 
         // (a) out parts, G rows per pass, each row's d targets ranked in
-        // registers; U passes' loads issued together.  Seed rows hold targets
-        // 0, 1, ... (both seed graphs); their absent slots sort last.
+        // registers (as 32-bit node ids: n < 2^32); U passes' loads issued
+        // together.  Seed rows hold targets 0, 1, ... (both seed graphs); their
+        // absent slots sort last.
         constexpr uint32_t U = 4;
         for (uint32_t r0 = 0; r0 < kRowsChunk; r0 += U * G) {
-            Id t[U];
+            uint32_t t[U];
             bool have[U];
             int64_t rrp[U];
 #pragma unroll
@@ -553,26 +646,24 @@ __global__ void __launch_bounds__(256) rows_kernel(const Id *E, const unsigned l
                 rrp[q] = __shfl_sync(kFull, rp, rj & 31u);
                 const uint64_t row = x0 + rj;
                 const bool act = used && rj < kRowsChunk && row < n;
-                t[q] = std::numeric_limits<Id>::max();
+                t[q] = 0xffffffffu;
                 have[q] = false;
                 if (act && row > d) {
-                    t[q] = E[2 * (seed_edges + (row - d - 1) * d + i) + 1];
+                    t[q] = (uint32_t)E[2 * (seed_edges + (row - d - 1) * d + i) + 1];
                     have[q] = true;
                 } else if (act && i < outdeg(row, d, seed_pre)) {
-                    t[q] = (Id)i;
+                    t[q] = i;
                     have[q] = true;
                 }
             }
 #pragma unroll
             for (uint32_t q = 0; q < U; ++q) {
                 uint32_t rank = 0;
-                for (uint32_t j = 0; j < d; ++j) {
-                    const Id o = __shfl_sync(kFull, t[q], (g * d + j) & 31u);
-                    rank += (o < t[q]) ? 1u : 0u;
-                }
+                for (uint32_t j = 0; j < d; ++j)
+                    rank += __shfl_sync(kFull, t[q], (g * d + j) & 31u) < t[q] ? 1u : 0u;
                 if (have[q]) {
                     const uint64_t pos = (uint64_t)rrp[q] + rank;
-                    if (pos < col_len) col[pos] = t[q];
+                    if (pos < col_len) col[pos] = (Id)t[q];
                 }
             }
         }
@@ -656,20 +747,47 @@ struct CsrLayout {
         seed_pre_off, heavy_off, giant_off, total;
     uint64_t r_tiles;               // radix tiles
     uint64_t heavy_cap, giant_cap;  // rows with in parts above kHeavyIn / kGiantIn items
+    uint32_t db, passes;            // digit bits and passes of the sort
+    uint64_t status_bytes;
+    bool status_in_col;             // status words in the column buffer's second half
 };
 
 // Graphs below 2^32 nodes: items pack (v, u) in 8 bytes.
 bool csr_supported(uint64_t n) { return n < (1ull << 32); }
 
-CsrLayout csr_layout(uint64_t n, uint32_t d, uint64_t n_edges)
+// Digit width of the sort: keys < n need bits(n - 1) bits (a pair with an id
+// outside the node range raises an error; its key, all ones in those bits, then
+// sorts last or among the keys n - 1).  The fewest passes of 8 or 9 bits, the
+// narrower digit on a tie (fewer counters per tile).
+void radix_digits(uint64_t n, uint32_t *db, uint32_t *passes)
 {
-    (void)n;
+    uint32_t bits = 1;
+    while (bits < 32 && ((n - 1) >> bits) != 0) ++bits;
+    // (10-bit digits -- the pass kernel's per-digit steps take two digits per
+    // thread when kRadixBuckets allows it -- measured twice as slow per pass as
+    // 8-bit ones at n = 2^30: two CTAs per SM and runs of ~6 items per digit
+    // and tile.  Three of them lost to four 8-bit passes, 306 against 238 ms.)
+    *db = 8;
+    *passes = (bits + 7) / 8;
+    if ((bits + 8) / 9 < *passes) {
+        *db = 9;
+        *passes = (bits + 8) / 9;
+    }
+}
+
+CsrLayout csr_layout(uint64_t n, uint32_t d, uint64_t n_edges, uint32_t id_bytes)
+{
     auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
     CsrLayout L{};
+    radix_digits(n, &L.db, &L.passes);
     L.r_tiles = (n_edges + kRadixTile - 1) / kRadixTile;
+    L.status_bytes = 8ull * (1u << L.db) * std::max<uint64_t>(L.r_tiles, 1);
+    // with 8-byte ids the column buffer (16 bytes per pair) holds the sort's
+    // second item array (8 per pair) and, behind it, the look-back words
+    L.status_in_col = id_bytes == 8 && L.status_bytes <= 8 * n_edges;
     uint64_t o = 0;
     L.items_off = o;    o += al(8 * std::max<uint64_t>(n_edges, 1));
-    L.status_off = o;   o += al(8 * kRadixBuckets * std::max<uint64_t>(L.r_tiles, 1));
+    L.status_off = o;   o += L.status_in_col ? 0 : al(L.status_bytes);
     L.hist_off = o;     o += al(8 * kMaxPasses * kRadixBuckets);
     L.base_off = o;     o += al(8 * kMaxPasses * kRadixBuckets);
     L.ctr_off = o;      o += 256;   // one tile counter per pass, then the two row lists'
@@ -689,14 +807,13 @@ CsrLayout csr_layout(uint64_t n, uint32_t d, uint64_t n_edges)
 // then one kernel per pass.  The last pass always lands in A.
 template <typename Id, uint32_t DB>
 int radix_sort(const Id *E, uint64_t m, uint64_t n, uint32_t passes, unsigned long long *A,
-               unsigned long long *B, unsigned char *scratch, const CsrLayout &L, uint32_t *err,
-               cudaStream_t s)
+               unsigned long long *B, unsigned long long *status, unsigned char *scratch,
+               const CsrLayout &L, uint32_t *err, cudaStream_t s)
 {
     constexpr uint32_t NB = 1u << DB;
     unsigned long long *hist = (unsigned long long *)(scratch + L.hist_off);
     unsigned long long *base = (unsigned long long *)(scratch + L.base_off);
     unsigned long long *ctr = (unsigned long long *)(scratch + L.ctr_off);
-    unsigned long long *status = (unsigned long long *)(scratch + L.status_off);
     const size_t smem = sizeof(RadixSmem<NB>);
     cudaError_t e = cudaFuncSetAttribute(radix_pass_kernel<Id, true, DB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -746,21 +863,22 @@ int csr_enqueue_t(const pa_params *prm, const GenPlan &p, const Id *E, int64_t *
     if (e != cudaSuccess) return set_cuda_error(e);
     seed_out_kernel<<<1, 256, 0, s>>>(d, prm->seed_mode, seed_out);
     seed_prefix_kernel<<<1, 32, 0, s>>>(seed_out, d, seed_pre);
-    uint32_t bits = 1;
-    while (bits < 32 && (n >> bits) != 0) ++bits;   // keys < n need bits(n) bits; kBadKey sorts last
-    // 9-bit digits when three passes cover the key (n < 2^27), else 8-bit ones
-    const uint32_t db = bits <= 27 ? 9u : 8u;
-    const uint32_t passes = (bits + db - 1) / db;
+    unsigned long long *status =
+        L.status_in_col ? reinterpret_cast<unsigned long long *>(col) + m
+                        : (unsigned long long *)(scratch + L.status_off);
     if (m > 0) {
-        const int rc = db == 9 ? radix_sort<Id, 9>(E, m, n, passes, A, B, scratch, L, err, s)
-                               : radix_sort<Id, 8>(E, m, n, passes, A, B, scratch, L, err, s);
+        int rc = PA_ERR_INVALID;
+        if (L.db == 9)
+            rc = radix_sort<Id, 9>(E, m, n, L.passes, A, B, status, scratch, L, err, s);
+        else
+            rc = radix_sort<Id, 8>(E, m, n, L.passes, A, B, status, scratch, L, err, s);
         if (rc != PA_OK) return rc;
     }
     const uint64_t col_len = 2 * m;
     if (p.wide) {
         // in parts and rowptr from the sorted items, the seed rows' out parts,
         // then the generated rows' out parts (ranked in shared memory)
-        in_sorted_kernel<Id, true><<<grid_for(m / 4 + 1, 256), 256, 0, s>>>(
+        in_sorted_kernel<Id><<<grid_for(m / 4 + 1, 256), 256, 0, s>>>(
             A, m, n, d, p.seed_edges, seed_pre, col, col_len, rowptr);
         out_part_kernel<Id><<<grid_for(n * d / 4 + 1, 256), 256, 0, s>>>(E, rowptr, col, n, d,
                                                                          p.seed_edges, col_len);
@@ -773,8 +891,8 @@ int csr_enqueue_t(const pa_params *prm, const GenPlan &p, const Id *E, int64_t *
         unsigned long long *giant = (unsigned long long *)(scratch + L.giant_off);
         e = cudaMemsetAsync(lists, 0, 16, s);
         if (e != cudaSuccess) return set_cuda_error(e);
-        in_sorted_kernel<Id, false><<<grid_for(m / 4 + 1, 256), 256, 0, s>>>(
-            A, m, n, d, p.seed_edges, seed_pre, col, col_len, rowptr);
+        rowptr_kernel<<<grid_for(m / 8 + 1, 256), 256, 0, s>>>(A, m, n, d, p.seed_edges,
+                                                                seed_pre, rowptr);
         const int grid = grid_for(n / kRowsChunk + 1, 256 / 32);
         rows_kernel<Id><<<grid, 256, 0, s>>>(E, A, m, rowptr, col, n, d, p.seed_edges, seed_pre,
                                              col_len, heavy, L.heavy_cap, giant, L.giant_cap,
@@ -800,7 +918,7 @@ int csr_enqueue(const pa_params *prm, const void *d_edges, int64_t *d_rowptr, vo
         return PA_ERR_NOT_SUPPORTED;
     if ((reinterpret_cast<uintptr_t>(d_col) & 15u) || (reinterpret_cast<uintptr_t>(d_scratch) & 15u))
         return PA_ERR_INVALID;
-    const CsrLayout L = csr_layout(prm->n, prm->d, p.n_edges);
+    const CsrLayout L = csr_layout(prm->n, prm->d, p.n_edges, p.id_bytes);
     if (scratch_bytes < L.total) return PA_ERR_CAPACITY;
     if (err_offset) *err_offset = L.err_off;
     if (p.id_bytes == 8)
@@ -827,7 +945,7 @@ int pa_csr_bytes(const pa_params *prm, uint64_t *rowptr_bytes, uint64_t *col_byt
         return PA_ERR_NOT_SUPPORTED;
     *rowptr_bytes = 8 * (prm->n + 1);
     *col_bytes = 2 * p.n_edges * p.id_bytes;
-    *scratch_bytes = csr_layout(prm->n, prm->d, p.n_edges).total;
+    *scratch_bytes = csr_layout(prm->n, prm->d, p.n_edges, p.id_bytes).total;
     return PA_OK;
 }
 

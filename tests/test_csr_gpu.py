@@ -21,6 +21,7 @@ CASES = [
     (6, 5, 0.5, 8, orc.SEED_CLIQUE, 32),             # seed graph only
     (2_000_000, 4, 0.0, 10, orc.SEED_CLIQUE, 64),    # five rows of ~1.6e6 in-edges
     (300_000, 16, 0.5, 11, orc.SEED_STAR_REF, 32),   # hubs of 512 .. 2^20 in-edges
+    (200_000, 8, 0.5, 12, orc.SEED_CLIQUE, 64),      # two 9-bit passes (10-bit: n above)
 ]
 
 

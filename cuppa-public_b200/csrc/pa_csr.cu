@@ -18,9 +18,9 @@
 // rows), with the in parts of hub rows copied by a block or the whole grid.
 // Items pack (v, u) in 8 bytes, so graphs of 2^32 nodes and more are refused.
 //
-// The sort reads the pairs twice and the items twice per pass: one histogram
-// kernel counts the digits of every pass while reading the pairs once, and each
-// pass is one kernel that keeps its tile on chip from the load to the store,
+// The sort reads the pairs once and the items twice per pass: one histogram
+// kernel counts the digits of every pass while it turns the pairs into items,
+// and each pass is one kernel that keeps its tile on chip from the load to the store,
 // taking each digit's offset from the tiles before it by decoupled
 // look-back (Merrill and Garland's single-pass prefix scan, as in Adinets and
 // Merrill's one-sweep radix sort) instead of a per-pass histogram and scan.
@@ -135,32 +135,30 @@ constexpr unsigned long long kLbValMask = (1ull << 56) - 1;
 constexpr uint32_t kLbEpochShift = 56;
 constexpr uint32_t kLbWindow = 4;   // predecessors read per look-back step
 
-// Item i of a pass.  The first pass reads the pairs (ids above the node range,
-// never produced by the generator, become kBadKey and raise an error).
-template <typename Id, bool First>
-__device__ __forceinline__ unsigned long long radix_item(const void *src, uint64_t i, uint64_t n,
-                                                         uint32_t *err)
+// Item of pair i (ids above the node range, never produced by the generator,
+// become kBadKey and raise an error).
+template <typename Id>
+__device__ __forceinline__ unsigned long long pair_item(const Id *E, uint64_t i, uint64_t n,
+                                                        uint32_t *err)
 {
-    if constexpr (First) {
-        const Id *E = reinterpret_cast<const Id *>(src);
-        const uint64_t u = (uint64_t)E[2 * i], v = (uint64_t)E[2 * i + 1];
-        if (u >= n || v >= n) {
-            atomicCAS(err, 0u, (uint32_t)PA_ERR_INVALID);
-            return (kBadKey << 32) | 0xffffffffull;
-        }
-        return (v << 32) | u;
-    } else {
-        return reinterpret_cast<const unsigned long long *>(src)[i];
+    const uint64_t u = (uint64_t)E[2 * i], v = (uint64_t)E[2 * i + 1];
+    if (u >= n || v >= n) {
+        atomicCAS(err, 0u, (uint32_t)PA_ERR_INVALID);
+        return (kBadKey << 32) | 0xffffffffull;
     }
+    return (v << 32) | u;
 }
 
-// Digit counts of every pass over all items (the pairs read once): per-block
-// shared counters, flushed with one global atomic per nonzero digit.  (Combining
-// a warp's equal digits with __match_any_sync first measured far slower than
-// the shared atomics it saves: 32 against ~5 ms at n = 10^8, d = 16.)
+// The items, in pair order, and the digit counts of every pass over them (the
+// pairs read once): per-block shared counters, flushed with one global atomic
+// per nonzero digit.  (Combining a warp's equal digits with __match_any_sync
+// first measured far slower than the shared atomics it saves: 32 against ~5 ms
+// at n = 10^8, d = 16.)  Writing the items here lets every pass read 8 bytes
+// per item instead of the first one reading the 16-byte pairs.
 template <typename Id, uint32_t DB>
 __global__ void __launch_bounds__(kRadixThreads) radix_hist_all_kernel(const Id *E, uint64_t n_items,
                                                                        uint64_t n, uint32_t passes,
+                                                                       unsigned long long *items,
                                                                        unsigned long long *hist,
                                                                        uint32_t *err)
 {
@@ -175,7 +173,12 @@ __global__ void __launch_bounds__(kRadixThreads) radix_hist_all_kernel(const Id 
 #pragma unroll
         for (uint32_t j = 0; j < U; ++j) {
             const uint64_t i = base + j * kRadixThreads + threadIdx.x;
-            key[j] = i < n_items ? (uint32_t)(radix_item<Id, true>(E, i, n, err) >> 32) : 0u;
+            key[j] = 0u;
+            if (i < n_items) {
+                const unsigned long long it = pair_item(E, i, n, err);
+                items[i] = it;
+                key[j] = (uint32_t)(it >> 32);
+            }
         }
 #pragma unroll
         for (uint32_t j = 0; j < U; ++j) {
@@ -218,9 +221,9 @@ struct RadixSmem {
 };
 
 // Three CTAs per SM up to 9-bit digits; two with the larger 10-bit counters.
-template <typename Id, bool First, uint32_t DB>
+template <uint32_t DB>
 __global__ void __launch_bounds__(kRadixThreads, DB > 9 ? 2 : 3) radix_pass_kernel(
-    const void *src, unsigned long long *dst, uint64_t n_items, uint32_t shift, uint64_t n,
+    const unsigned long long *src, unsigned long long *dst, uint64_t n_items, uint32_t shift,
     const unsigned long long *digit_base, unsigned long long *status, uint32_t epoch,
     unsigned long long *tile_ctr, uint64_t spin_limit_ns, uint32_t *err)
 {
@@ -253,7 +256,7 @@ __global__ void __launch_bounds__(kRadixThreads, DB > 9 ? 2 : 3) radix_pass_kern
 #pragma unroll
         for (uint32_t q = 0; q < kRadixRounds / 2; ++q) {
             const uint32_t k = wo + (h + q) * 32 + lane;
-            its[q] = k < tcount ? radix_item<Id, First>(src, tb + k, n, err) : 0ull;
+            its[q] = k < tcount ? src[tb + k] : 0ull;
         }
 #pragma unroll
         for (uint32_t q = 0; q < kRadixRounds / 2; ++q) {
@@ -815,31 +818,23 @@ int radix_sort(const Id *E, uint64_t m, uint64_t n, uint32_t passes, unsigned lo
     unsigned long long *base = (unsigned long long *)(scratch + L.base_off);
     unsigned long long *ctr = (unsigned long long *)(scratch + L.ctr_off);
     const size_t smem = sizeof(RadixSmem<NB>);
-    cudaError_t e = cudaFuncSetAttribute(radix_pass_kernel<Id, true, DB>,
+    cudaError_t e = cudaFuncSetAttribute(radix_pass_kernel<DB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(radix_pass_kernel<Id, false, DB>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // status words of an earlier call must not read as this call's
     if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, 8 * (uint64_t)NB * L.r_tiles, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(hist, 0, 8 * kMaxPasses * kRadixBuckets, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(ctr, 0, 8 * kMaxPasses, s);
     if (e != cudaSuccess) return set_cuda_error(e);
+    // pass q reads what pass q - 1 wrote; the histogram kernel writes the
+    // items where pass 0 reads them, so that the last pass lands in A
+    auto buf = [&](uint32_t k) { return (passes - k) % 2 == 0 ? A : B; };   // pass k - 1's output
     radix_hist_all_kernel<Id, DB><<<grid_for(m / 4 + 1, kRadixThreads, 2), kRadixThreads, 0, s>>>(
-        E, m, n, passes, hist, err);
+        E, m, n, passes, buf(0), hist, err);
     radix_base_kernel<DB><<<1, 32, 0, s>>>(hist, passes, base);
     const unsigned tiles = (unsigned)L.r_tiles;
-    for (uint32_t q = 0; q < passes; ++q) {
-        const uint32_t shift = DB * q;
-        unsigned long long *dst = ((passes - 1 - q) % 2 == 0) ? A : B;
-        const void *src = q == 0 ? (const void *)E : (const void *)(((passes - q) % 2 == 0) ? A : B);
-        if (q == 0)
-            radix_pass_kernel<Id, true, DB><<<tiles, kRadixThreads, smem, s>>>(
-                src, dst, m, shift, n, base + q * NB, status, q + 1, ctr + q, 2000000000ull, err);
-        else
-            radix_pass_kernel<Id, false, DB><<<tiles, kRadixThreads, smem, s>>>(
-                src, dst, m, shift, n, base + q * NB, status, q + 1, ctr + q, 2000000000ull, err);
-    }
+    for (uint32_t q = 0; q < passes; ++q)
+        radix_pass_kernel<DB><<<tiles, kRadixThreads, smem, s>>>(
+            buf(q), buf(q + 1), m, DB * q, base + q * NB, status, q + 1, ctr + q, 2000000000ull, err);
     e = cudaGetLastError();
     return e == cudaSuccess ? PA_OK : set_cuda_error(e);
 }

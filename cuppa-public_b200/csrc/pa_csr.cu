@@ -111,9 +111,9 @@ __global__ void seed_out_kernel(uint32_t d, uint32_t seed_mode, uint32_t *seed_o
 // the node range and no per-row sorting.
 //
 // A pass sorts 8 or 9 key bits (the fewest passes for the key).  Its
-// kernel claims tiles of 6144 items in order from a counter; a tile's 512
-// threads load 12 items each and park them in shared memory, rank them stably
-// -- each of 16 warps walks its 384 items in order, 32 at a time, with
+// kernel claims tiles of 8192 items in order from a counter; a tile's 512
+// threads load 16 items each and park them in shared memory, rank them stably
+// -- each of 16 warps walks its 512 items in order, 32 at a time, with
 // __match_any_sync for equal digits and 16-bit per-warp counters in shared
 // memory -- publish the tile's count of every digit, and look back over the
 // tiles before it (their counts, or the running total the nearest finished
@@ -122,7 +122,7 @@ __global__ void seed_out_kernel(uint32_t d, uint32_t seed_mode, uint32_t *seed_o
 // ---------------------------------------------------------------------------
 constexpr uint32_t kRadixThreads = 512, kRadixWarps = kRadixThreads / 32;
 constexpr uint32_t kRadixBuckets = 512;   // the widest digit in use: 9 bits
-constexpr uint32_t kRadixRounds = 12;     // items per lane per tile
+constexpr uint32_t kRadixRounds = 16;     // items per lane per tile
 constexpr uint32_t kRadixTile = kRadixThreads * kRadixRounds;
 constexpr uint32_t kMaxPasses = 4;
 constexpr unsigned long long kBadKey = 0xffffffffull;   // sorts after every node id
@@ -220,9 +220,13 @@ struct RadixSmem {
     unsigned long long tile;
 };
 
-// Three CTAs per SM up to 9-bit digits; two with the larger 10-bit counters.
+// Two CTAs per SM (84 KB of shared memory each at 9-bit digits, 64 registers).
+// Measured at n = 2^30, d = 4 (C3 CSR) and n = 10^8, d = 16 (C2): 8,192-item
+// tiles at two CTAs 224-227 / 75.6 ms; 6,144-item tiles at three CTAs and 40
+// registers (which spill) 231 / 76.0 ms; 7,168, 9,216 and 10,240-item tiles at
+// two CTAs 231 / 74.2, 238 / 76.8 and 241 / 77.1 ms.
 template <uint32_t DB>
-__global__ void __launch_bounds__(kRadixThreads, DB > 9 ? 2 : 3) radix_pass_kernel(
+__global__ void __launch_bounds__(kRadixThreads, 2) radix_pass_kernel(
     const unsigned long long *src, unsigned long long *dst, uint64_t n_items, uint32_t shift,
     const unsigned long long *digit_base, unsigned long long *status, uint32_t epoch,
     unsigned long long *tile_ctr, uint64_t spin_limit_ns, uint32_t *err)
@@ -768,8 +772,9 @@ void radix_digits(uint64_t n, uint32_t *db, uint32_t *passes)
     while (bits < 32 && ((n - 1) >> bits) != 0) ++bits;
     // (10-bit digits -- the pass kernel's per-digit steps take two digits per
     // thread when kRadixBuckets allows it -- measured twice as slow per pass as
-    // 8-bit ones at n = 2^30: two CTAs per SM and runs of ~6 items per digit
-    // and tile.  Three of them lost to four 8-bit passes, 306 against 238 ms.)
+    // 8-bit ones at n = 2^30 with 6,144-item tiles: 88 KB of shared memory,
+    // 64 registers, runs of ~6 items per digit and tile.  Three of them lost
+    // to four 8-bit passes, 306 against 238 ms.)
     *db = 8;
     *passes = (bits + 7) / 8;
     if ((bits + 8) / 9 < *passes) {

@@ -15,13 +15,13 @@
 //   4. out part: each generated row's d targets ranked in registers and stored;
 //      the seed rows' targets are 0, 1, ... (both seed graphs).
 // Steps 3 and 4 run in one row writer for d <= 32 (a warp writes 32 whole
-// rows), with the in parts of hub rows copied by a block or the whole grid.
+// rows), with the in parts of hub rows copied in pieces spread over all warps.
 // Items pack (v, u) in 8 bytes, so graphs of 2^32 nodes and more are refused.
 //
 // The sort reads the pairs once and the items twice per pass: one histogram
 // kernel counts the digits of every pass while it turns the pairs into items,
-// and each pass is one kernel that keeps its tile on chip from the load to the store,
-// taking each digit's offset from the tiles before it by decoupled
+// and each pass is one kernel that keeps its tile on chip from the load to the
+// store, taking each digit's offset from the tiles before it by decoupled
 // look-back (Merrill and Garland's single-pass prefix scan, as in Adinets and
 // Merrill's one-sweep radix sort) instead of a per-pass histogram and scan.
 #include <algorithm>
@@ -37,55 +37,21 @@ namespace {
 
 constexpr uint32_t kFull = 0xffffffffu;
 // ---------------------------------------------------------------------------
-// Out parts.
+// Seed rows' out parts for the path of d > 32 (rows_kernel writes them for
+// d <= 32; csr_out_wide writes the generated rows): the seed rows' out-edges go
+// to targets 0, 1, ... in order in both seed graphs (CLIQUE row v: 0..v-1;
+// STAR_REF row d: 0..d-1), so an edge's position in its row is its target.
 // ---------------------------------------------------------------------------
 template <typename Id>
-__global__ void out_part_kernel(const Id *E, const int64_t *rowptr, Id *col, uint64_t n, uint32_t d,
-                                uint64_t seed_edges, uint64_t col_len)
+__global__ void seed_out_part_kernel(const Id *E, const int64_t *rowptr, Id *col, uint64_t n,
+                                     uint64_t seed_edges, uint64_t col_len)
 {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-    const uint64_t w0 = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    // seed rows: the seed rows' out-edges go to targets 0, 1, ... in order in
-    // both seed graphs (CLIQUE row v: 0..v-1; STAR_REF row d: 0..d-1), so an
-    // edge's position in its row is its target
-    for (uint64_t e = w0 * 32 + lane; e < seed_edges; e += warps * 32) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < seed_edges; e += stride) {
         const uint64_t u = (uint64_t)E[2 * e], t = (uint64_t)E[2 * e + 1];
         if (u < n && t < u) {
             const uint64_t pos = (uint64_t)rowptr[u] + t;
             if (pos < col_len) col[pos] = E[2 * e + 1];
-        }
-    }
-    if (d > 32) return;   // generated rows of d > 32: csr_out_wide (pa_wide.cu)
-    const uint32_t G = 32u / d;
-    const uint32_t g = lane / d, i = lane - g * d;
-    const bool used = lane < G * d;
-    const uint64_t rows = n - (d + 1);
-    // U warp passes per step, their loads issued together
-    constexpr uint32_t U = 4;
-    for (uint64_t r0 = w0 * G * U; r0 < rows; r0 += warps * G * U) {
-        Id dst[U];
-        int64_t start[U];
-#pragma unroll
-        for (uint32_t q = 0; q < U; ++q) {
-            const uint64_t row = r0 + q * G + g;
-            const bool act = used && row < rows;
-            dst[q] = act ? E[2 * (seed_edges + row * d + i) + 1] : (Id)0;
-            start[q] = act ? rowptr[row + d + 1] : 0;
-        }
-#pragma unroll
-        for (uint32_t q = 0; q < U; ++q) {
-            const uint64_t row = r0 + q * G + g;
-            const bool act = used && row < rows;
-            uint32_t rank = 0;
-            for (uint32_t j = 0; j < d; ++j) {
-                const Id o = __shfl_sync(kFull, dst[q], (g * d + j) & 31u);
-                rank += (o < dst[q]) ? 1u : 0u;
-            }
-            if (act) {
-                const uint64_t pos = (uint64_t)start[q] + rank;
-                if (pos < col_len) col[pos] = dst[q];
-            }
         }
     }
 }
@@ -552,12 +518,14 @@ __global__ void __launch_bounds__(256) rowptr_kernel(const unsigned long long *i
 //
 // Row x's in part is sorted items [lb(x), lb(x+1)), lb(x) = rowptr[x] -
 // outprefix(x); entry k of it (item index) goes to col[outprefix(x+1) + k].
-// A row whose in part is longer than kHeavyIn items is left to
-// heavy_in_kernel (listed here), so that hub rows do not hold one warp.
+// A row whose in part is longer than kHeavyIn items is listed here and its in
+// part copied in pieces of kPiece items spread over all warps (heavy_scan_kernel,
+// heavy_in_kernel), so that hub rows -- up to every item at p = 0 -- hold no
+// single warp or block.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kRowsChunk = 32;        // rows per warp step: one per lane
 constexpr uint64_t kHeavyIn = 512;         // longest in part a row warp copies
-constexpr uint64_t kGiantIn = 1ull << 20;  // longer: copied by the whole grid
+constexpr uint32_t kPiece = 512;           // items per piece of a longer one
 
 __device__ __forceinline__ uint64_t clamp_items(int64_t v, uint64_t n_items)
 {
@@ -604,7 +572,6 @@ __global__ void __launch_bounds__(256) rows_kernel(const Id *E, const unsigned l
                                                    uint64_t n, uint32_t d, uint64_t seed_edges,
                                                    const int64_t *seed_pre, uint64_t col_len,
                                                    unsigned long long *heavy, uint64_t heavy_cap,
-                                                   unsigned long long *giant, uint64_t giant_cap,
                                                    unsigned long long *ctr)
 {
     const uint32_t lane = threadIdx.x & 31u;
@@ -629,13 +596,8 @@ __global__ void __launch_bounds__(256) rows_kernel(const Id *E, const unsigned l
         const bool heavy_row = row_ok && lb1 - lb > kHeavyIn;
         if (heavy_row) {
             // listed in any order: every entry's place is fixed by its index
-            if (lb1 - lb > kGiantIn) {
-                const unsigned long long s = atomicAdd(ctr + 1, 1ull);
-                if (s < giant_cap) giant[s] = x;
-            } else {
-                const unsigned long long s = atomicAdd(ctr, 1ull);
-                if (s < heavy_cap) heavy[s] = x;
-            }
+            const unsigned long long slot = atomicAdd(ctr, 1ull);
+            if (slot < heavy_cap) heavy[slot] = x;
         }
 
         // (a) out parts, G rows per pass, each row's d targets ranked in
@@ -694,8 +656,77 @@ __global__ void __launch_bounds__(256) rows_kernel(const Id *E, const unsigned l
     }
 }
 
-// In parts of the listed rows: a heavy row per block (block stride over the
-// list), then each giant row by the whole grid.
+// Row x's in part: sorted items [lb, lb1), entry k at col[base + k].
+struct InPart {
+    uint64_t lb, lb1, base;
+};
+
+__device__ __forceinline__ InPart in_part(uint64_t x, const int64_t *rowptr, uint64_t n_items,
+                                          uint32_t d, uint64_t seed_edges, const int64_t *seed_pre)
+{
+    InPart r;
+    r.base = outprefix(x + 1, d, seed_edges, seed_pre);
+    r.lb = clamp_items(rowptr[x] - (int64_t)outprefix(x, d, seed_edges, seed_pre), n_items);
+    r.lb1 = clamp_items(rowptr[x + 1] - (int64_t)r.base, n_items);
+    if (r.lb1 < r.lb) r.lb1 = r.lb;
+    return r;
+}
+
+// The first piece of every listed row: pref[h] = pieces of rows 0..h-1 of the
+// list, pref[K] = all pieces (one block; the list holds at most one entry per
+// kHeavyIn items).
+__global__ void __launch_bounds__(1024) heavy_scan_kernel(const unsigned long long *heavy,
+                                                          uint64_t heavy_cap,
+                                                          const unsigned long long *ctr,
+                                                          const int64_t *rowptr, uint64_t n,
+                                                          uint32_t d, uint64_t seed_edges,
+                                                          const int64_t *seed_pre,
+                                                          uint64_t n_items,
+                                                          unsigned long long *pref)
+{
+    __shared__ unsigned long long wsum[32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint64_t K = min((uint64_t)ctr[0], heavy_cap);
+    unsigned long long carry = 0;
+    for (uint64_t h0 = 0; h0 < K; h0 += 1024) {
+        const uint64_t h = h0 + threadIdx.x;
+        unsigned long long pc = 0;
+        if (h < K && heavy[h] < n) {
+            const InPart r = in_part(heavy[h], rowptr, n_items, d, seed_edges, seed_pre);
+            pc = (r.lb1 - r.lb + kPiece - 1) / kPiece;
+        }
+        unsigned long long x = pc;   // inclusive scan over the block
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(kFull, x, o);
+            if (lane >= (uint32_t)o) x += y;
+        }
+        if (lane == 31) wsum[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            unsigned long long w = wsum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long y = __shfl_up_sync(kFull, w, o);
+                if (lane >= (uint32_t)o) w += y;
+            }
+            wsum[lane] = w;
+        }
+        __syncthreads();
+        const unsigned long long before = warp > 0 ? wsum[warp - 1] : 0ull;
+        if (h < K) pref[h] = carry + before + x - pc;
+        carry += wsum[31];
+        __syncthreads();   // wsum is rewritten by the next chunk
+    }
+    if (threadIdx.x == 0) pref[K] = carry;
+}
+
+// In parts of the listed rows, in pieces of kPiece items: a warp takes runs of
+// kPieceRun consecutive pieces (over all listed rows, in list order), finds the
+// row of its first piece by binary search over pref and copies each piece with
+// all 32 lanes (kPiece / 32 items each, loads issued together).
+constexpr uint32_t kPieceRun = 16;
+
 template <typename Id>
 __global__ void __launch_bounds__(256) heavy_in_kernel(const unsigned long long *items,
                                                        uint64_t n_items, const int64_t *rowptr,
@@ -704,39 +735,49 @@ __global__ void __launch_bounds__(256) heavy_in_kernel(const unsigned long long 
                                                        uint64_t col_len,
                                                        const unsigned long long *heavy,
                                                        uint64_t heavy_cap,
-                                                       const unsigned long long *giant,
-                                                       uint64_t giant_cap,
-                                                       const unsigned long long *ctr)
+                                                       const unsigned long long *ctr,
+                                                       const unsigned long long *pref)
 {
-    const uint64_t n_heavy = min((uint64_t)ctr[0], heavy_cap);
-    const uint64_t n_giant = min((uint64_t)ctr[1], giant_cap);
-    auto copy_row = [&](uint64_t x, uint64_t first, uint64_t stride) {
-        if (x >= n) return;
-        const uint64_t lb = clamp_items(rowptr[x] - (int64_t)outprefix(x, d, seed_edges, seed_pre),
-                                        n_items);
-        const uint64_t lb1 = clamp_items(
-            rowptr[x + 1] - (int64_t)outprefix(x + 1, d, seed_edges, seed_pre), n_items);
-        const uint64_t base = outprefix(x + 1, d, seed_edges, seed_pre);
-        constexpr uint32_t U = 4;
-        for (uint64_t k0 = lb + first; k0 < lb1; k0 += U * stride) {
-            unsigned long long it[U];
+    constexpr uint32_t PL = kPiece / 32;   // items per lane per piece
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    const uint64_t w0 = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint64_t K = min((uint64_t)ctr[0], heavy_cap);
+    if (K == 0) return;
+    const uint64_t T = pref[K];
+    for (uint64_t t0 = w0 * kPieceRun; t0 < T; t0 += warps * kPieceRun) {
+        // the last h with pref[h] <= t0 (pref[0] = 0, pref is non-decreasing)
+        uint64_t lo = 0, hi = K;
+        while (hi - lo > 1) {
+            const uint64_t mid = lo + (hi - lo) / 2;
+            if (pref[mid] <= t0) lo = mid;
+            else hi = mid;
+        }
+        uint64_t h = lo, next = pref[h + 1];
+        InPart r{0, 0, 0};
+        if (heavy[h] < n) r = in_part(heavy[h], rowptr, n_items, d, seed_edges, seed_pre);
+        const uint64_t t1 = min(t0 + kPieceRun, T);
+        for (uint64_t t = t0; t < t1; ++t) {
+            while (t >= next && h + 1 < K) {   // rows of one piece or more: a few steps
+                ++h;
+                next = pref[h + 1];
+                r = heavy[h] < n ? in_part(heavy[h], rowptr, n_items, d, seed_edges, seed_pre)
+                                 : InPart{0, 0, 0};
+            }
+            const uint64_t k0 = r.lb + (t - pref[h]) * kPiece;
+            unsigned long long it[PL];
 #pragma unroll
-            for (uint32_t q = 0; q < U; ++q) {
-                const uint64_t k = k0 + q * stride;
-                it[q] = k < lb1 ? items[k] : 0ull;
+            for (uint32_t q = 0; q < PL; ++q) {
+                const uint64_t k = k0 + q * 32 + lane;
+                it[q] = k < r.lb1 ? items[k] : 0ull;
             }
 #pragma unroll
-            for (uint32_t q = 0; q < U; ++q) {
-                const uint64_t k = k0 + q * stride, pos = base + k;
-                if (k < lb1 && pos < col_len) col[pos] = (Id)(it[q] & 0xffffffffull);
+            for (uint32_t q = 0; q < PL; ++q) {
+                const uint64_t k = k0 + q * 32 + lane, pos = r.base + k;
+                if (k < r.lb1 && pos < col_len) col[pos] = (Id)(it[q] & 0xffffffffull);
             }
         }
-    };
-    for (uint64_t h = blockIdx.x; h < n_heavy; h += gridDim.x)
-        copy_row(heavy[h], threadIdx.x, blockDim.x);
-    const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    for (uint64_t h = 0; h < n_giant; ++h)
-        copy_row(giant[h], gt, (uint64_t)gridDim.x * blockDim.x);
+    }
 }
 
 int grid_for(uint64_t items, uint32_t threads, uint32_t per_sm = 8)
@@ -751,9 +792,9 @@ int grid_for(uint64_t items, uint32_t threads, uint32_t per_sm = 8)
 
 struct CsrLayout {
     uint64_t items_off, status_off, hist_off, base_off, ctr_off, err_off, seed_out_off,
-        seed_pre_off, heavy_off, giant_off, total;
+        seed_pre_off, heavy_off, pref_off, total;
     uint64_t r_tiles;               // radix tiles
-    uint64_t heavy_cap, giant_cap;  // rows with in parts above kHeavyIn / kGiantIn items
+    uint64_t heavy_cap;             // rows with in parts above kHeavyIn items
     uint32_t db, passes;            // digit bits and passes of the sort
     uint64_t status_bytes;
     bool status_in_col;             // status words in the column buffer's second half
@@ -798,15 +839,15 @@ CsrLayout csr_layout(uint64_t n, uint32_t d, uint64_t n_edges, uint32_t id_bytes
     L.status_off = o;   o += L.status_in_col ? 0 : al(L.status_bytes);
     L.hist_off = o;     o += al(8 * kMaxPasses * kRadixBuckets);
     L.base_off = o;     o += al(8 * kMaxPasses * kRadixBuckets);
-    L.ctr_off = o;      o += 256;   // one tile counter per pass, then the two row lists'
+    L.ctr_off = o;      o += 256;   // one tile counter per pass, then the hub rows'
     L.err_off = o;      o += 256;
     L.seed_out_off = o; o += al(4 * (d + 1));
     L.seed_pre_off = o; o += al(8 * (d + 2));
     // more than cap rows cannot each hold more than kHeavyIn of the n_edges items
     L.heavy_cap = n_edges / (kHeavyIn + 1) + 1;
-    L.giant_cap = n_edges / (kGiantIn + 1) + 1;
+
     L.heavy_off = o;    o += al(8 * L.heavy_cap);
-    L.giant_off = o;    o += al(8 * L.giant_cap);
+    L.pref_off = o;     o += al(8 * (L.heavy_cap + 1));
     L.total = o;
     return L;
 }
@@ -880,26 +921,28 @@ int csr_enqueue_t(const pa_params *prm, const GenPlan &p, const Id *E, int64_t *
         // then the generated rows' out parts (ranked in shared memory)
         in_sorted_kernel<Id><<<grid_for(m / 4 + 1, 256), 256, 0, s>>>(
             A, m, n, d, p.seed_edges, seed_pre, col, col_len, rowptr);
-        out_part_kernel<Id><<<grid_for(n * d / 4 + 1, 256), 256, 0, s>>>(E, rowptr, col, n, d,
-                                                                         p.seed_edges, col_len);
+        seed_out_part_kernel<Id><<<grid_for(p.seed_edges, 256), 256, 0, s>>>(E, rowptr, col, n,
+                                                                             p.seed_edges, col_len);
         const int rc = gen::csr_out_wide(p.id_bytes, E, rowptr, col, n, d, p.seed_edges, col_len, s);
         if (rc != PA_OK) return rc;
     } else {
         // rowptr, then whole rows (the hub rows' in parts listed and copied last)
         unsigned long long *lists = (unsigned long long *)(scratch + L.ctr_off) + kMaxPasses;
         unsigned long long *heavy = (unsigned long long *)(scratch + L.heavy_off);
-        unsigned long long *giant = (unsigned long long *)(scratch + L.giant_off);
-        e = cudaMemsetAsync(lists, 0, 16, s);
+        unsigned long long *pref = (unsigned long long *)(scratch + L.pref_off);
+        e = cudaMemsetAsync(lists, 0, 8, s);
         if (e != cudaSuccess) return set_cuda_error(e);
         rowptr_kernel<<<grid_for(m / 8 + 1, 256), 256, 0, s>>>(A, m, n, d, p.seed_edges,
                                                                 seed_pre, rowptr);
         const int grid = grid_for(n / kRowsChunk + 1, 256 / 32);
         rows_kernel<Id><<<grid, 256, 0, s>>>(E, A, m, rowptr, col, n, d, p.seed_edges, seed_pre,
-                                             col_len, heavy, L.heavy_cap, giant, L.giant_cap,
-                                             lists);
-        heavy_in_kernel<Id><<<grid_for(m / 8 + 1, 256), 256, 0, s>>>(
-            A, m, rowptr, col, n, d, p.seed_edges, seed_pre, col_len, heavy, L.heavy_cap, giant,
-            L.giant_cap, lists);
+                                             col_len, heavy, L.heavy_cap, lists);
+        heavy_scan_kernel<<<1, 1024, 0, s>>>(heavy, L.heavy_cap, lists, rowptr, n, d,
+                                              p.seed_edges, seed_pre, m, pref);
+        // one warp per run of kPieceRun pieces; at most m / kPiece + (listed rows) pieces
+        heavy_in_kernel<Id><<<grid_for(m / (kPiece * kPieceRun) + 1, 256 / 32), 256, 0, s>>>(
+            A, m, rowptr, col, n, d, p.seed_edges, seed_pre, col_len, heavy, L.heavy_cap, lists,
+            pref);
     }
     e = cudaGetLastError();
     return e == cudaSuccess ? PA_OK : set_cuda_error(e);

@@ -1,8 +1,8 @@
 """Device CSR build vs the oracle's CSR (bit-exact: rowptr and every row's
-sorted column list).  Shapes cover the three ways a row's in part is copied:
-by the warp that writes the row (<= 512 entries), by one block (hub rows up to
-2^20 entries: the hubs at p = 0.2 and d = 16) and by the whole grid (longer:
-the seed nodes at p = 0 and n = 2 * 10^6)."""
+sorted column list).  Shapes cover both ways a row's in part is copied: by the
+warp that writes the row (<= 512 entries), and in 512-entry pieces spread over
+all warps for longer ones -- the hubs at p = 0.2 and d = 16, and the seed nodes
+at p = 0 and n = 2 * 10^6 (~1.6e6 entries each, thousands of pieces)."""
 import numpy as np
 import pytest
 
@@ -20,7 +20,7 @@ CASES = [
     (5000, 32, 0.3, 7, orc.SEED_STAR_REF, 32),
     (6, 5, 0.5, 8, orc.SEED_CLIQUE, 32),             # seed graph only
     (2_000_000, 4, 0.0, 10, orc.SEED_CLIQUE, 64),    # five rows of ~1.6e6 in-edges
-    (300_000, 16, 0.5, 11, orc.SEED_STAR_REF, 32),   # hubs of 512 .. 2^20 in-edges
+    (300_000, 16, 0.5, 11, orc.SEED_STAR_REF, 32),   # hubs of 512 .. 4600 in-edges
     (200_000, 8, 0.5, 12, orc.SEED_CLIQUE, 64),      # two 9-bit passes (10-bit: n above)
 ]
 

@@ -21,7 +21,13 @@ CASES = [
     (6, 5, 0.5, 8, orc.SEED_CLIQUE, 32),             # seed graph only
     (2_000_000, 4, 0.0, 10, orc.SEED_CLIQUE, 64),    # five rows of ~1.6e6 in-edges
     (300_000, 16, 0.5, 11, orc.SEED_STAR_REF, 32),   # hubs of 512 .. 4600 in-edges
-    (200_000, 8, 0.5, 12, orc.SEED_CLIQUE, 64),      # two 9-bit passes (10-bit: n above)
+    (200_000, 8, 0.5, 12, orc.SEED_CLIQUE, 64),      # two 9-bit passes
+    # d not dividing 32: idle lanes in every out-part pass of the row writer
+    (40000, 3, 0.5, 13, orc.SEED_CLIQUE, 32),
+    (30000, 7, 0.3, 14, orc.SEED_STAR_REF, 64),
+    (20000, 20, 0.6, 15, orc.SEED_CLIQUE, 32),
+    (10000, 31, 0.5, 16, orc.SEED_STAR_REF, 64),
+    (50000, 2, 0.1, 17, orc.SEED_CLIQUE, 32),
 ]
 
 

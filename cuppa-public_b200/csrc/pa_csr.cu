@@ -538,8 +538,8 @@ __device__ __forceinline__ uint32_t outdeg(uint64_t x, uint32_t d, const int64_t
     return x <= (uint64_t)d ? (uint32_t)(seed_pre[x + 1] - seed_pre[x]) : d;
 }
 
-// Copy sorted items [a, b) (all of key v or, in a row warp, of keys in the
-// warp's rows) into their in part places; U loads per lane in flight.
+// Copy sorted items [a, b) -- the in parts of some of a row warp's rows -- into
+// their places in col; U loads per lane in flight.
 template <typename Id>
 __device__ __forceinline__ void copy_in_items(const unsigned long long *items, uint64_t a, uint64_t b,
                                               uint32_t lane, uint64_t n, uint32_t d,

@@ -625,13 +625,22 @@ __global__ void __launch_bounds__(256) rows_kernel(const Id *E, const unsigned l
                     have[q] = true;
                 }
             }
+            // the U passes' ranks in one loop: U independent shuffles per step
+            uint32_t rank[U];
+#pragma unroll
+            for (uint32_t q = 0; q < U; ++q) rank[q] = 0;
+            const uint32_t gb = g * d;
+#pragma unroll 2
+            for (uint32_t j = 0; j < d; ++j) {
+                const uint32_t src = (gb + j) & 31u;
+#pragma unroll
+                for (uint32_t q = 0; q < U; ++q)
+                    rank[q] += __shfl_sync(kFull, t[q], src) < t[q] ? 1u : 0u;
+            }
 #pragma unroll
             for (uint32_t q = 0; q < U; ++q) {
-                uint32_t rank = 0;
-                for (uint32_t j = 0; j < d; ++j)
-                    rank += __shfl_sync(kFull, t[q], (g * d + j) & 31u) < t[q] ? 1u : 0u;
                 if (have[q]) {
-                    const uint64_t pos = (uint64_t)rrp[q] + rank;
+                    const uint64_t pos = (uint64_t)rrp[q] + rank[q];
                     if (pos < col_len) col[pos] = (Id)t[q];
                 }
             }

@@ -580,15 +580,24 @@ __global__ void __launch_bounds__(256) rows_kernel(const Id *E, const unsigned l
     const uint32_t G = 32u / d;   // rows per out part pass, d lanes each
     const uint32_t g = lane / d, i = lane - g * d;
     const bool used = lane < G * d;
-    for (uint64_t x0 = w0 * kRowsChunk; x0 < n; x0 += warps * kRowsChunk) {
+    const uint64_t step = warps * kRowsChunk;
+    // rowptr of each chunk's rows is loaded one chunk ahead
+    int64_t rp_next = 0, rp1_next = 0;
+    if (w0 * kRowsChunk + lane < n) {
+        rp_next = rowptr[w0 * kRowsChunk + lane];
+        rp1_next = rowptr[w0 * kRowsChunk + lane + 1];
+    }
+    for (uint64_t x0 = w0 * kRowsChunk; x0 < n; x0 += step) {
         // lane j: row x0 + j, its rowptr and its in part's item range
         const uint64_t x = x0 + lane;
         const bool row_ok = x < n;
-        int64_t rp = 0;
+        const int64_t rp = row_ok ? rp_next : 0, rp1 = row_ok ? rp1_next : 0;
+        if (x + step < n) {
+            rp_next = rowptr[x + step];
+            rp1_next = rowptr[x + step + 1];
+        }
         uint64_t lb = n_items, lb1 = n_items;
         if (row_ok) {
-            rp = rowptr[x];
-            const int64_t rp1 = rowptr[x + 1];
             lb = clamp_items(rp - (int64_t)outprefix(x, d, seed_edges, seed_pre), n_items);
             lb1 = clamp_items(rp1 - (int64_t)outprefix(x + 1, d, seed_edges, seed_pre), n_items);
             if (lb1 < lb) lb1 = lb;
@@ -598,6 +607,18 @@ __global__ void __launch_bounds__(256) rows_kernel(const Id *E, const unsigned l
             // listed in any order: every entry's place is fixed by its index
             const unsigned long long slot = atomicAdd(ctr, 1ull);
             if (slot < heavy_cap) heavy[slot] = x;
+        }
+        uint32_t hv = __ballot_sync(kFull, heavy_row);
+        uint64_t a = __shfl_sync(kFull, lb, 0);
+        const uint64_t end = __shfl_sync(kFull, lb1, 31);
+        // without hub rows the chunk's in parts are items [a, end): their first
+        // kPre * 32 loads go out now, beside the out parts' loads below
+        constexpr uint32_t kPre = 4;
+        unsigned long long pre[kPre];
+#pragma unroll
+        for (uint32_t q = 0; q < kPre; ++q) {
+            const uint64_t k = a + q * 32 + lane;
+            pre[q] = hv == 0 && k < end ? items[k] : ~0ull;
         }
 
         // (a) out parts, G rows per pass, each row's d targets ranked in
@@ -647,9 +668,18 @@ __global__ void __launch_bounds__(256) rows_kernel(const Id *E, const unsigned l
         }
 
         // (b) in parts of the chunk's rows, the heavy rows' ranges skipped
-        uint32_t hv = __ballot_sync(kFull, heavy_row);
-        uint64_t a = __shfl_sync(kFull, lb, 0);
-        const uint64_t end = __shfl_sync(kFull, lb1, 31);
+        if (hv == 0) {
+#pragma unroll
+            for (uint32_t q = 0; q < kPre; ++q) {
+                const uint64_t k = a + q * 32 + lane;
+                const uint64_t v = pre[q] >> 32;
+                if (k < end && v < n) {
+                    const uint64_t pos = outprefix(v + 1, d, seed_edges, seed_pre) + k;
+                    if (pos < col_len) col[pos] = (Id)(pre[q] & 0xffffffffull);
+                }
+            }
+            a = min(a + kPre * 32, end);
+        }
         while (true) {
             uint64_t b = end, next = end;
             if (hv) {

@@ -973,6 +973,7 @@ def run_served(args):
                    "parallelism": f"requests round-robin over {world} servers (one per rank)"
                    if world > 1 else "single", "output": fig["output"]},
         "p50_ms": fig["p50_ms"], "p99_ms": fig["p99_ms"], "max_ms": fig["max_ms"],
+        "express_sized": fig["express_sized"], "bulk_sized": fig["bulk_sized"],
         "requests_per_s": fig["served_requests_per_s"],
         "offered_requests_per_s": fig["offered_requests_per_s"],
         "offered_edges_per_s": fig["offered_edges_per_s"], "all_ok": ok,

@@ -26,8 +26,7 @@
 //    current) and cached under the context's ID.  A context created anew --
 //    after cudaDeviceReset, or after the primary context was released and
 //    retained again -- has a new ID, so its first call looks the address up
-//    again instead of reusing one from a context that no longer exists.
-//    Make that first call before any stream capture begins;
+//    again instead of reusing one from a context that no longer exists;
 //  * each call clears the part of the array it uses before launching, so the
 //    contents a previous call left behind never leak into the result.
 #include <cuda.h>

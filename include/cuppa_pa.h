@@ -180,9 +180,8 @@ int pa_generate_finish(const void *d_scratch, pa_stats *out, void *stream);
  * work.  The first call in a CUDA context looks the array's address up with
  * cudaGetSymbolAddress (with that context's device current) and caches it under
  * the context's ID, so a context created anew after cudaDeviceReset is looked
- * up again: make that first call before any stream capture begins.  All calls on a device share the
- * array, so calls whose GPU work overlaps race on it: issue them on one stream
- * or serialize them.  Each call clears what it uses, generates on `stream`,
+ * up again.  All calls on a device share the array, so calls whose GPU work
+ * overlaps race on it: issue them on one stream or serialize them.  Each call clears what it uses, generates on `stream`,
  * waits for it, fills *stats (may be NULL) and returns the device status. */
 #define PA_NOALLOC_SCRATCH_BYTES (16u << 20)
 int pa_generate_noalloc(const pa_params *prm, void *d_edges, uint64_t edges_bytes,

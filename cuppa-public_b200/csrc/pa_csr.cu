@@ -913,7 +913,10 @@ int radix_sort(const Id *E, uint64_t m, uint64_t n, uint32_t passes, unsigned lo
     // pass q reads what pass q - 1 wrote; the histogram kernel writes the
     // items where pass 0 reads them, so that the last pass lands in A
     auto buf = [&](uint32_t k) { return (passes - k) % 2 == 0 ? A : B; };   // pass k - 1's output
-    radix_hist_all_kernel<Id, DB><<<grid_for(m / 4 + 1, kRadixThreads, 2), kRadixThreads, 0, s>>>(
+    // four 512-thread blocks per SM (24 registers, 8 KB of counters each): at
+    // n = 10^8, d = 16 the kernel took 8.44 ms with two blocks per SM, 5.96 ms
+    // with four
+    radix_hist_all_kernel<Id, DB><<<grid_for(m / 4 + 1, kRadixThreads, 4), kRadixThreads, 0, s>>>(
         E, m, n, passes, buf(0), hist, err);
     radix_base_kernel<DB><<<1, 32, 0, s>>>(hist, passes, base);
     const unsigned tiles = (unsigned)L.r_tiles;
